@@ -1,0 +1,277 @@
+/*
+ * rb_capi.h -- the C ABI of the B200 progressive-LOD path.
+ *
+ * The reference drives its LOD pipelines through the C++ plugin interface
+ * ILodPipeline (include/remo/ILodPipeline.h:118-146); each implementation
+ * launches NVRTC-compiled kernels with positional void* argument arrays
+ * (src/pipelines/RemolodPipeline.cpp:346-347, :403-405). This header is the
+ * boundary that replaces those launches: plain C, POD structs, device pointers
+ * as uint64_t, no C++ or torch types. The C++ host (remobench_b200/host/) keeps
+ * the ILodPipeline interface and forwards to these entry points; Python binds
+ * them with ctypes.
+ *
+ * Threading: a context is not thread-safe; calls are ordered on its stream.
+ * Errors: every entry point returns rb_status; rb_last_error() has the text.
+ * Device-side capacity limits never fault: they set flags in rb_stats.
+ */
+#ifndef RB_CAPI_H
+#define RB_CAPI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RB_ABI_VERSION 1u
+
+typedef int32_t rb_status;
+enum {
+    RB_OK = 0,
+    RB_ERR_INVALID_ARG = 1,
+    RB_ERR_CUDA = 2,          /* a CUDA call failed; the text names it */
+    RB_ERR_OUT_OF_MEMORY = 3,
+    RB_ERR_STATE = 4,         /* call out of order (e.g. build before allocate) */
+    RB_ERR_RING = 5,          /* ring depth does not match (RemolodPipeline.cpp:315-328) */
+    RB_ERR_CAPACITY = 6,      /* a request beyond a configured maximum */
+    RB_ERR_NO_DEVICE = 7,
+    RB_ERR_UNSUPPORTED = 8
+};
+
+/* Pipeline ids registered by the reference (src/shell/App.cpp:85-95). */
+enum { RB_PIPELINE_REMOLOD = 0, RB_PIPELINE_SIMLOD = 1, RB_PIPELINE_FLAT = 2 };
+
+/* Voxel representative rule. LOWEST_INDEX: the cell's colour comes from the
+ * lowest global point index that reaches it in the batch (deterministic).
+ * FIRST_COME: from whichever point arrives first, as the reference does
+ * (kernels/remolod/remolod_octree.cu:116-138). */
+enum { RB_VOXEL_LOWEST_INDEX = 0, RB_VOXEL_FIRST_COME = 1 };
+
+/* Overflow flag bits reported in rb_stats.overflow_flags. */
+enum {
+    RB_OVF_SPILLED = 1u,   /* spill list full (remolod_octree.cu:76) */
+    RB_OVF_BACKLOG = 2u,   /* new-voxel table full (:26) */
+    RB_OVF_SPILLING = 4u,  /* spilling-node list full (:40) */
+    RB_OVF_ARENA = 8u,     /* grid/chunk arena full */
+    RB_OVF_TABLES = 64u,   /* chunk-table pool full */
+    RB_OVF_DIRTY = 128u,   /* accumulate dirty list full */
+    RB_OVF_DRAWLIST = 256u /* render draw list full (remolod_render.cu:22) */
+};
+
+/* 16-byte point (include/remo/HostDeviceCommon.h:15-18): rgba with r in the low byte. */
+typedef struct rb_point {
+    float x, y, z;
+    uint32_t color;
+} rb_point;
+
+/* Constants of kernels/remolod/remolod_structures.cuh:12-25 and
+ * remolod_octree.cu:26-76 as run-time parameters. */
+typedef struct rb_config {
+    uint32_t struct_size;            /* sizeof(rb_config) */
+    uint32_t pipeline;               /* RB_PIPELINE_* */
+    int32_t device;                  /* CUDA device ordinal */
+    uint32_t max_nodes;              /* 200000 */
+    uint32_t max_points_per_node;    /* 50000 */
+    uint32_t points_per_chunk;       /* 1000 */
+    uint32_t max_expand_iters;       /* 20 */
+    uint32_t ring_slots;             /* 50 */
+    uint32_t slot_capacity;          /* 1000000 points per ring slot */
+    uint32_t max_batches_per_build;  /* 20 */
+    float time_budget_ms;            /* 10; 0 = no wall-clock budget */
+    uint32_t voxel_mode;             /* RB_VOXEL_* */
+    uint32_t accumulate;             /* fold Accumulate into every build (remolod) */
+    uint32_t spilled_capacity;       /* 10,000,000 */
+    uint32_t spilling_nodes_capacity;/* 100,000 */
+    uint32_t drawlist_capacity;      /* 131072 */
+    uint64_t safety_margin;          /* 200,000,000 bytes */
+    uint32_t use_graphs;             /* capture each batch's kernels in a CUDA graph */
+    uint32_t reserved[7];
+} rb_config;
+
+/* CloudMeta (include/remo/PointSource.h:16-32), headless subset. */
+typedef struct rb_cloud_meta {
+    uint64_t num_points;
+    float box_min[3];
+    float box_max[3];
+} rb_cloud_meta;
+
+/* BatchView (include/remo/PointSource.h:43-67). slots is a device pointer to
+ * num_slots * slot_capacity points; batch_sizes is host memory (num_slots
+ * entries), read at the call. */
+typedef struct rb_batch_view {
+    uint64_t slots;
+    const uint32_t* batch_sizes;
+    uint32_t num_batches_uploaded;
+    uint32_t slot_capacity;
+    uint32_t num_slots;
+    uint32_t num_batches_total;
+} rb_batch_view;
+
+/* SharedUniforms subset (include/remo/HostDeviceCommon.h:28-60). Matrices are
+ * row-major: clip = M * (x, y, z, 1). */
+typedef struct rb_frame {
+    float width, height;
+    float transform[16];
+    float transform_frozen[16];
+    float box_min[3], box_max[3];
+    float lod_pixel_budget;          /* 128 (src/shell/App.h:50-62) */
+    int32_t point_size;              /* 1 */
+    uint32_t enable_edl;
+    float edl_strength;              /* 0.4 */
+    uint64_t frame_counter;
+} rb_frame;
+
+typedef struct rb_build_result {
+    uint32_t batches_consumed;       /* Stats::batchletIndex after the call */
+    uint32_t batches_this_call;
+    uint32_t more;                   /* batches remain in the cloud */
+    uint32_t mem_capacity_reached;
+    float device_ms;                 /* CUDA-event time of the call's GPU work */
+    uint32_t pad;
+} rb_build_result;
+
+/* PipelineStats (include/remo/ILodPipeline.h:88-111) plus the reference's
+ * Stats (kernels/simlod/HostDeviceInterface.h:51-76) and diagnostics. */
+typedef struct rb_stats {
+    uint64_t num_points;
+    uint64_t num_voxels;
+    uint64_t num_points_ingested;
+    uint32_t num_nodes;
+    uint32_t num_inner;
+    uint32_t num_leaves;
+    uint32_t num_nonempty_leaves;
+    uint32_t max_depth;
+    uint32_t max_points_per_node;
+    uint32_t num_chunks_points;
+    uint32_t num_chunks_voxels;
+    uint32_t batchlet_index;
+    uint32_t counter_underflows;
+    uint64_t num_allocated_chunks;
+    uint64_t chunk_pool_size;
+    uint64_t persistent_offset;      /* the reference store's allocator offset */
+    uint64_t persistent_capacity;
+    uint64_t bytes_allocated;        /* device bytes this context holds */
+    uint64_t dropped_points;
+    uint64_t expand_iters;
+    uint64_t nodes_split;
+    uint64_t spilled_points;
+    uint32_t num_grids;
+    uint32_t overflow_flags;         /* RB_OVF_* */
+    uint32_t mem_capacity_reached;
+    uint32_t node_capacity_reached;
+    uint32_t num_visible_nodes;      /* last render */
+    uint32_t pad;
+    uint64_t num_visible_samples;
+} rb_stats;
+
+typedef struct rb_render_result {
+    uint32_t draw_items;
+    uint32_t drawlist_overflow;
+    uint64_t draw_samples;
+    float device_ms;
+    uint32_t pad;
+} rb_render_result;
+
+/* AccumGlobals (include/remo/RemoAccum.h:33-41). */
+typedef struct rb_accum_globals {
+    uint64_t morton_watermark;
+    uint64_t num_accumulated;
+    uint64_t sum_leaf_counts;
+    uint32_t points_folded;
+    uint32_t num_leaves_folded;
+    uint32_t inner_with_sums;
+    uint32_t pad;
+} rb_accum_globals;
+
+/* Exact per-node sums (NodeAccum, include/remo/RemoAccum.h:24-31, in integers):
+ * s1 = Σq, s2 = Σqqᵀ as 128-bit (xx xy xz yy yz zz), c1/c2 = Σ and Σ² of the
+ * 8-bit r, g, b channels; q is the point's 28-bit octree coordinate relative to
+ * the node, clamped to [0, 2^(28-level)]. */
+typedef struct rb_accum {
+    uint64_t s1[3];
+    uint64_t s2_lo[6];
+    uint64_t s2_hi[6];
+    uint64_t c1[3];
+    uint64_t c2[3];
+    uint32_t count;                  /* watermark: slots folded so far */
+    uint32_t last_touched_batch;
+    uint32_t state;
+    uint32_t pad;
+} rb_accum;
+
+/* One node of the pool, for parity dumps. */
+typedef struct rb_node_info {
+    int32_t child[8];
+    uint32_t counter;
+    uint32_t num_points;
+    uint32_t level;
+    uint32_t X, Y, Z;
+    uint32_t has_grid;
+    uint32_t num_voxels;
+    uint32_t num_point_chunks;
+    uint32_t num_voxel_chunks;
+    uint32_t is_leaf;
+} rb_node_info;
+
+uint32_t rb_abi_version(void);
+const char* rb_status_string(rb_status s);
+void rb_config_defaults(rb_config* cfg);
+
+/* Construction (no device allocation: ILodPipeline::initPrograms "must NOT
+ * allocate", wiki/01_Overview.md:142-160) and teardown. */
+rb_status rb_create(const rb_config* cfg, struct rb_ctx** out);
+void rb_destroy(struct rb_ctx* ctx);
+const char* rb_last_error(const struct rb_ctx* ctx);
+rb_status rb_set_stream(struct rb_ctx* ctx, void* cuda_stream);
+
+/* ILodPipeline::allocate / release (RemolodPipeline.cpp:105-212): sizes the
+ * node pool, arena and scratch from the cloud and the byte budget. */
+rb_status rb_allocate(struct rb_ctx* ctx, const rb_cloud_meta* meta, uint64_t budget_bytes);
+void rb_release(struct rb_ctx* ctx);
+
+/* ILodPipeline::reset + the reset kernel (kernels/remolod/remolod_reset.cu:23-87). */
+rb_status rb_reset(struct rb_ctx* ctx);
+
+/* ILodPipeline::build for the progressive pipelines (RemolodPipeline.cpp:296-438):
+ * consumes up to max_batches_per_build uploaded batches from the ring within
+ * the time budget, then (remolod) runs Accumulate. */
+rb_status rb_build(struct rb_ctx* ctx, const rb_batch_view* view, rb_build_result* out);
+
+/* End-to-end ingest of host points: streams them through a device ring with
+ * copies overlapped on a second stream, n points in batches of batch_size
+ * (<= slot_capacity), Accumulate after the last batch. */
+rb_status rb_ingest_host(struct rb_ctx* ctx, const rb_point* points, uint64_t n, uint32_t batch_size,
+                         rb_build_result* out);
+
+/* kernel_accumulate + kernel_accum_verify (remolod_accum.cu:47-233). */
+rb_status rb_accumulate(struct rb_ctx* ctx, uint32_t batch_index, rb_accum_globals* out);
+
+/* ILodPipeline::render (RemolodPipeline.cpp:559-601) into a headless device
+ * framebuffer: fb_dev holds width*height uint64 (depth<<32 | rgba); rgba_dev
+ * (optional, 0 = none) receives the resolved colours. force_large_dev
+ * (optional) marks nodes the LOD cut must open (Refinement). */
+rb_status rb_render(struct rb_ctx* ctx, const rb_frame* frame, uint64_t fb_dev, uint64_t rgba_dev,
+                    uint64_t force_large_dev, rb_render_result* out);
+
+/* The flat pipeline (kernels/flat/flat_render.cu:9-76): every point of a
+ * resident cloud. */
+rb_status rb_render_flat(struct rb_ctx* ctx, const rb_frame* frame, uint64_t points_dev, uint64_t n,
+                         uint64_t fb_dev, uint64_t rgba_dev, rb_render_result* out);
+
+/* ILodPipeline::stats (+ the stats sweep, remolod_octree.cu:1271-1310). */
+rb_status rb_read_stats(struct rb_ctx* ctx, rb_stats* out);
+
+/* Parity dumps. */
+rb_status rb_read_nodes(struct rb_ctx* ctx, rb_node_info* out, uint32_t capacity, uint32_t* count);
+rb_status rb_read_node_points(struct rb_ctx* ctx, uint32_t node, rb_point* pts, uint32_t* idx,
+                              uint32_t capacity, uint32_t* count);
+rb_status rb_read_node_voxels(struct rb_ctx* ctx, uint32_t node, rb_point* vox, uint32_t capacity,
+                              uint32_t* count);
+rb_status rb_read_node_grid(struct rb_ctx* ctx, uint32_t node, uint32_t* words65536);
+rb_status rb_read_accums(struct rb_ctx* ctx, rb_accum* out, uint32_t capacity, uint32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

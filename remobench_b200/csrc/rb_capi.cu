@@ -1,0 +1,840 @@
+// The C ABI (include/rb_capi.h): context lifetime, buffer sizing, and the host
+// side of each stage -- the launch sequencing RemolodPipeline performs in the
+// reference (src/pipelines/RemolodPipeline.cpp:105-601), on one CUDA stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rb_capi.h"
+#include "rb_kernels.h"
+#include "rb_state.h"
+
+using rb::Counters;
+using rb::Dev;
+using rb::kNone;
+
+struct rb_ctx {
+    rb_config cfg{};
+    std::string err;
+    int device = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t evStart = nullptr, evStop = nullptr;
+    bool allocated = false;
+    Dev d{};
+    std::vector<void*> allocs;
+    uint64_t bytes = 0;
+    Counters* hostCtr = nullptr;  // pinned mirror
+    rb::SweepStats* hostSweep = nullptr;
+    rb::AccumGlobals* hostAccum = nullptr;
+    rb::RenderScratch* hostRs = nullptr;
+    // render scratch
+    uint8_t* vis = nullptr;
+    uint8_t* large = nullptr;
+    uint32_t* items = nullptr;
+    rb::RenderScratch* rs = nullptr;
+    unsigned long long* fbTmp = nullptr;
+    uint64_t fbTmpPixels = 0;
+    // host-ingest ring
+    rb::Point* ingestRing = nullptr;
+    uint32_t ingestSlots = 0;
+    cudaEvent_t slotFree[4] = {};
+    cudaEvent_t slotFull[4] = {};
+    // cloud
+    uint64_t numPoints = 0;
+    uint32_t batchesConsumed = 0;
+    bool accumAll = true;         // next accumulate must visit every node
+    uint32_t lastVisibleNodes = 0;
+    uint64_t lastVisibleSamples = 0;
+};
+
+namespace {
+
+rb_status fail(rb_ctx* c, rb_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+#define RB_CUDA(c, call)                                                                      \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail((c), RB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+rb_status devAlloc(rb_ctx* c, T** p, uint64_t count, const char* what) {
+    void* q = nullptr;
+    const uint64_t bytes = std::max<uint64_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, RB_ERR_OUT_OF_MEMORY,
+                    std::string("cudaMalloc failed for ") + what + " (" + std::to_string(bytes >> 20) + " MB)");
+    }
+    c->allocs.push_back(q);
+    c->bytes += bytes;
+    *p = static_cast<T*>(q);
+    return RB_OK;
+}
+
+uint32_t nextPow2(uint64_t v) {
+    uint64_t m = 1;
+    while (m < v) m <<= 1;
+    return (uint32_t)std::min<uint64_t>(m, 1ull << 31);
+}
+
+int pointGrid(const rb_ctx* c, uint64_t n) {
+    const uint64_t blocks = (n + 255) / 256;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)c->numSMs * 8));
+}
+
+rb_status readCounters(rb_ctx* c) {
+    RB_CUDA(c, cudaMemcpyAsync(c->hostCtr, c->d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream));
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return RB_OK;
+}
+
+// One batch through addBatch's phases (remolod_octree.cu:940-1060). Returns
+// RB_OK with *stopped set when the memory check refused the batch.
+rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIndex, bool* stopped) {
+    const Dev& d = c->d;
+    cudaStream_t s = c->stream;
+    *stopped = false;
+    if (c->hostCtr->overflowFlags & rb::kOvfBacklog) {
+        // an overflowed batch left table entries its list could not name
+        RB_CUDA(c, cudaMemsetAsync(d.hashKeys, 0xFF, ((size_t)d.hashMask + 1) * 8, s));
+        RB_CUDA(c, cudaMemsetAsync(d.hashVals, 0xFF, ((size_t)d.hashMask + 1) * 8, s));
+    }
+    rb::launchBatchBegin(d, s);
+    rb::launchCountFirst(d, pts, n, pointGrid(c, n), s);
+    const int fixedGrid = c->numSMs * 4;
+    for (uint32_t iter = 1;; iter++) {
+        rb_status st = readCounters(c);
+        if (st != RB_OK) return st;
+        if (c->hostCtr->batchStop) {
+            *stopped = true;
+            return RB_OK;
+        }
+        if (c->hostCtr->numSpill == 0) break;
+        const uint32_t stamp = (batchIndex << 5) | iter;
+        rb::launchSplit(d, stamp, s);
+        rb::launchSpillCopy(d, fixedGrid, s);
+        if (iter >= c->cfg.max_expand_iters) break;
+        rb::launchRecount(d, pts, n, stamp, pointGrid(c, n), s);
+    }
+    const uint64_t work = n;
+    rb::launchVoxSample(d, pts, n, pointGrid(c, work), s);
+    rb::launchVoxCommit(d, fixedGrid, s);
+    rb::launchAllocChunks(d, fixedGrid, s);
+    rb::launchInsert(d, pts, n, pointGrid(c, work), s);
+    rb::launchVoxStore(d, fixedGrid, s);
+    rb::launchBatchEnd(d, n, s);
+    RB_CUDA(c, cudaGetLastError());
+    return RB_OK;
+}
+
+__global__ void k_build_begin(Counters* c) {
+    c->buildStamp += 1;
+    c->numDirty = 0;
+}
+
+rb_status accumulate(rb_ctx* c, uint32_t batchIndex) {
+    const Dev& d = c->d;
+    // sumLeafCounts .. innerWithSums restart per launch (RemolodPipeline.cpp:251-256)
+    RB_CUDA(c, cudaMemsetAsync(reinterpret_cast<uint8_t*>(d.accumGlobals) + 16, 0, 20, c->stream));
+    rb::launchAccumulate(d, batchIndex, c->accumAll ? 0 : 1, c->numSMs * 8, c->stream);
+    rb::launchAccumVerify(d, c->numSMs * 2, c->stream);
+    RB_CUDA(c, cudaGetLastError());
+    c->accumAll = false;
+    return RB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t rb_abi_version(void) { return RB_ABI_VERSION; }
+
+const char* rb_status_string(rb_status s) {
+    switch (s) {
+        case RB_OK: return "ok";
+        case RB_ERR_INVALID_ARG: return "invalid argument";
+        case RB_ERR_CUDA: return "CUDA error";
+        case RB_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case RB_ERR_STATE: return "call out of order";
+        case RB_ERR_RING: return "ring depth mismatch";
+        case RB_ERR_CAPACITY: return "beyond a configured capacity";
+        case RB_ERR_NO_DEVICE: return "no CUDA device";
+        case RB_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+void rb_config_defaults(rb_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->struct_size = sizeof(rb_config);
+    cfg->pipeline = RB_PIPELINE_REMOLOD;
+    cfg->device = 0;
+    cfg->max_nodes = 200000;
+    cfg->max_points_per_node = 50000;
+    cfg->points_per_chunk = 1000;
+    cfg->max_expand_iters = 20;
+    cfg->ring_slots = 50;
+    cfg->slot_capacity = 1000000;
+    cfg->max_batches_per_build = 20;
+    cfg->time_budget_ms = 10.0f;
+    cfg->voxel_mode = RB_VOXEL_LOWEST_INDEX;
+    cfg->accumulate = 1;
+    cfg->spilled_capacity = 10000000;
+    cfg->spilling_nodes_capacity = 100000;
+    cfg->drawlist_capacity = 131072;
+    cfg->safety_margin = 200000000ull;
+    cfg->use_graphs = 0;
+}
+
+rb_status rb_create(const rb_config* cfg, rb_ctx** out) {
+    if (!cfg || !out || cfg->struct_size != sizeof(rb_config)) return RB_ERR_INVALID_ARG;
+    if (cfg->pipeline > RB_PIPELINE_FLAT || cfg->max_nodes < 9 || cfg->points_per_chunk == 0 ||
+        cfg->slot_capacity == 0 || cfg->ring_slots == 0 || cfg->max_expand_iters == 0 ||
+        cfg->max_expand_iters > 31 || cfg->voxel_mode > RB_VOXEL_FIRST_COME ||
+        cfg->max_nodes > (1u << 21))
+        return RB_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return RB_ERR_NO_DEVICE;
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) return RB_ERR_INVALID_ARG;
+    rb_ctx* c = new rb_ctx();
+    c->cfg = *cfg;
+    c->device = cfg->device;
+    *out = c;
+    return RB_OK;
+}
+
+void rb_release(rb_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void* p : c->allocs) cudaFree(p);
+    c->allocs.clear();
+    if (c->fbTmp) cudaFree(c->fbTmp);
+    c->bytes = 0;
+    if (c->hostCtr) cudaFreeHost(c->hostCtr);
+    if (c->hostSweep) cudaFreeHost(c->hostSweep);
+    if (c->hostAccum) cudaFreeHost(c->hostAccum);
+    if (c->hostRs) cudaFreeHost(c->hostRs);
+    c->hostCtr = nullptr;
+    c->hostSweep = nullptr;
+    c->hostAccum = nullptr;
+    c->hostRs = nullptr;
+    for (int i = 0; i < 4; i++) {
+        if (c->slotFree[i]) cudaEventDestroy(c->slotFree[i]);
+        if (c->slotFull[i]) cudaEventDestroy(c->slotFull[i]);
+        c->slotFree[i] = c->slotFull[i] = nullptr;
+    }
+    c->d = Dev{};
+    c->vis = c->large = nullptr;
+    c->items = nullptr;
+    c->rs = nullptr;
+    c->fbTmp = nullptr;
+    c->fbTmpPixels = 0;
+    c->ingestRing = nullptr;
+    c->allocated = false;
+}
+
+void rb_destroy(rb_ctx* c) {
+    if (!c) return;
+    rb_release(c);
+    if (c->evStart) cudaEventDestroy(c->evStart);
+    if (c->evStop) cudaEventDestroy(c->evStop);
+    if (c->copyStream) cudaStreamDestroy(c->copyStream);
+    if (c->ownStream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* rb_last_error(const rb_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+rb_status rb_set_stream(rb_ctx* c, void* stream) {
+    if (!c) return RB_ERR_INVALID_ARG;
+    if (c->ownStream && c->stream) cudaStreamDestroy(c->stream);
+    c->stream = static_cast<cudaStream_t>(stream);
+    c->ownStream = false;
+    return RB_OK;
+}
+
+rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
+    if (!c || !meta) return RB_ERR_INVALID_ARG;
+    if (meta->num_points == 0) return fail(c, RB_ERR_INVALID_ARG, "cloud is empty");
+    rb_release(c);
+    RB_CUDA(c, cudaSetDevice(c->device));
+    cudaDeviceProp prop{};
+    RB_CUDA(c, cudaGetDeviceProperties(&prop, c->device));
+    c->numSMs = prop.multiProcessorCount;
+    if (!c->stream) {
+        RB_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->ownStream = true;
+    }
+    if (!c->copyStream) RB_CUDA(c, cudaStreamCreateWithFlags(&c->copyStream, cudaStreamNonBlocking));
+    if (!c->evStart) RB_CUDA(c, cudaEventCreate(&c->evStart));
+    if (!c->evStop) RB_CUDA(c, cudaEventCreate(&c->evStop));
+
+    const rb_config& cfg = c->cfg;
+    c->numPoints = meta->num_points;
+    Dev& d = c->d;
+    d.maxNodes = cfg.max_nodes;
+    d.maxPointsPerNode = cfg.max_points_per_node;
+    d.ppc = cfg.points_per_chunk;
+    d.maxExpandIters = cfg.max_expand_iters;
+    d.voxelMode = cfg.voxel_mode;
+    d.safetyMargin = cfg.safety_margin;
+    for (int a = 0; a < 3; a++) d.boxMin[a] = meta->box_min[a];
+    // remolod_octree.cu:1148-1149
+    const float sx = meta->box_max[0] - meta->box_min[0], sy = meta->box_max[1] - meta->box_min[1],
+                sz = meta->box_max[2] - meta->box_min[2];
+    d.octreeSize = std::max(std::max(sx, sy), sz);
+    if (!(d.octreeSize > 0.0f)) return fail(c, RB_ERR_INVALID_ARG, "empty bounding box");
+
+    if (cfg.pipeline == RB_PIPELINE_FLAT) {
+        // flat keeps no tree: render scratch only
+        if (devAlloc(c, &c->rs, 1, "render scratch") != RB_OK) return RB_ERR_OUT_OF_MEMORY;
+        RB_CUDA(c, cudaMallocHost(&c->hostRs, sizeof(rb::RenderScratch)));
+        RB_CUDA(c, cudaMallocHost(&c->hostCtr, sizeof(Counters)));
+        c->allocated = true;
+        return RB_OK;
+    }
+
+    // Store sizing (RemolodPipeline.cpp:118-157): 48 B/pt appetite, 512 MB
+    // floor, clamped to what the budget leaves after the ring and fixed parts.
+    size_t freeB = 0, totalB = 0;
+    RB_CUDA(c, cudaMemGetInfo(&freeB, &totalB));
+    if (budget == 0) budget = (uint64_t)(freeB * 0.85);
+    const uint64_t batches = (meta->num_points + cfg.slot_capacity - 1) / cfg.slot_capacity;
+    const uint64_t ringBytes = std::min<uint64_t>(cfg.ring_slots, batches) * cfg.slot_capacity * 16ull;
+    const uint64_t available = budget > ringBytes ? budget - ringBytes : 0;
+    const uint64_t fixedBytes = (uint64_t)cfg.max_nodes * (152 + 112) + (512ull << 20);
+    const uint64_t minPersistent = 512ull << 20;
+    if (available < fixedBytes + minPersistent)
+        return fail(c, RB_ERR_OUT_OF_MEMORY,
+                    "not enough device memory: needs at least " +
+                        std::to_string((fixedBytes + minPersistent) >> 20) + " MB, " +
+                        std::to_string(available >> 20) + " MB available");
+    uint64_t want = std::max<uint64_t>((uint64_t)(48.0 * (double)meta->num_points), minPersistent);
+    d.persistentCapacity = std::min<uint64_t>(want, available - fixedBytes);
+
+    // The arena: the reference store's worst case plus the wider point chunks
+    // (indices kept beside the points): at most 1.25 x its capacity.
+    const uint64_t ptChunkBytes = ((uint64_t)d.ppc * 20ull + 15ull) & ~15ull;
+    d.ptChunkUnits = (uint32_t)(ptChunkBytes / 16ull);
+    d.vxChunkUnits = d.ppc;
+    uint64_t arenaBytes = d.persistentCapacity + d.persistentCapacity / 4 + (64ull << 20);
+    arenaBytes = std::min<uint64_t>(arenaBytes, (uint64_t)UINT32_MAX * 16ull);
+    d.arenaUnits = (uint32_t)(arenaBytes / 16ull);
+    const uint64_t maxChunks = arenaBytes / (uint64_t)(d.vxChunkUnits * 16ull) + 1;
+    d.maxPtChunks = (uint32_t)std::min<uint64_t>(maxChunks, UINT32_MAX);
+    d.tablePoolCap = (uint32_t)std::min<uint64_t>(128ull * cfg.max_nodes + 4ull * maxChunks, 1ull << 31);
+    d.spillCap = cfg.spilled_capacity;
+    d.spillingCap = cfg.spilling_nodes_capacity;
+    const uint32_t hashSize = nextPow2(4ull * cfg.slot_capacity);
+    d.hashMask = hashSize - 1;
+    d.newCap = hashSize / 2;
+
+    const uint32_t N = cfg.max_nodes;
+    rb_status st = RB_OK;
+#define ALLOC(ptr, n, what) \
+    if ((st = devAlloc(c, &(ptr), (n), (what))) != RB_OK) { rb_release(c); return st; }
+    ALLOC(d.child, (uint64_t)N * 8, "node children");
+    ALLOC(d.counter, N, "node counters");
+    ALLOC(d.numPoints, N, "node point counts");
+    ALLOC(d.level, N, "node levels");
+    ALLOC(d.nodeX, N, "node X");
+    ALLOC(d.nodeY, N, "node Y");
+    ALLOC(d.nodeZ, N, "node Z");
+    ALLOC(d.grid, N, "node grids");
+    ALLOC(d.numVoxels, N, "node voxel counts");
+    ALLOC(d.numVoxelsStored, N, "node stored voxel counts");
+    ALLOC(d.numPointChunks, N, "node point chunk counts");
+    ALLOC(d.numVoxelChunks, N, "node voxel chunk counts");
+    ALLOC(d.ptTableOff, N, "point table offsets");
+    ALLOC(d.ptTableCap, N, "point table capacities");
+    ALLOC(d.vxTableOff, N, "voxel table offsets");
+    ALLOC(d.vxTableCap, N, "voxel table capacities");
+    ALLOC(d.splitIter, N, "split stamps");
+    ALLOC(d.dirtyStamp, N, "dirty stamps");
+    ALLOC(d.accum, N, "accumulators");
+    ALLOC(d.dirtyList, N, "dirty list");
+    ALLOC(d.arena, arenaBytes, "the arena (grids and chunks)");
+    ALLOC(d.tablePool, d.tablePoolCap, "chunk tables");
+    ALLOC(d.chunkQueue, d.maxPtChunks, "chunk queue");
+    ALLOC(d.leafOf, cfg.slot_capacity, "per-point leaves");
+    ALLOC(d.spillPts, d.spillCap, "spilled points");
+    ALLOC(d.spillIdx, d.spillCap, "spilled point indices");
+    ALLOC(d.spillLeaf, d.spillCap, "spilled point leaves");
+    ALLOC(d.spillNodes, nextPow2(d.spillingCap), "spilling nodes");
+    ALLOC(d.splitRecs, d.spillingCap, "split records");
+    ALLOC(d.hashKeys, hashSize, "voxel cell table keys");
+    ALLOC(d.hashVals, hashSize, "voxel cell table values");
+    ALLOC(d.hashNew, d.newCap, "new voxel cells");
+    ALLOC(d.hashNewNode, d.newCap, "new voxel nodes");
+    ALLOC(d.hashNewSlot, d.newCap, "new voxel slots");
+    ALLOC(d.ctr, 1, "counters");
+    ALLOC(d.sweep, 1, "sweep stats");
+    ALLOC(d.accumGlobals, 1, "accumulator globals");
+    ALLOC(c->vis, N, "visible flags");
+    ALLOC(c->large, N, "large flags");
+    ALLOC(c->items, std::max<uint32_t>(cfg.drawlist_capacity, 1), "draw list");
+    ALLOC(c->rs, 1, "render scratch");
+    c->ingestSlots = 3;
+    ALLOC(c->ingestRing, (uint64_t)c->ingestSlots * cfg.slot_capacity, "ingest ring");
+#undef ALLOC
+    RB_CUDA(c, cudaMemsetAsync(d.hashKeys, 0xFF, (size_t)hashSize * 8, c->stream));
+    RB_CUDA(c, cudaMemsetAsync(d.hashVals, 0xFF, (size_t)hashSize * 8, c->stream));
+    RB_CUDA(c, cudaMemsetAsync(d.ctr, 0, sizeof(Counters), c->stream));
+    RB_CUDA(c, cudaMemsetAsync(d.accumGlobals, 0, sizeof(rb::AccumGlobals), c->stream));
+    RB_CUDA(c, cudaMallocHost(&c->hostCtr, sizeof(Counters)));
+    std::memset(c->hostCtr, 0, sizeof(Counters));
+    RB_CUDA(c, cudaMallocHost(&c->hostSweep, sizeof(rb::SweepStats)));
+    RB_CUDA(c, cudaMallocHost(&c->hostAccum, sizeof(rb::AccumGlobals)));
+    RB_CUDA(c, cudaMallocHost(&c->hostRs, sizeof(rb::RenderScratch)));
+    for (uint32_t i = 0; i < c->ingestSlots; i++) {
+        RB_CUDA(c, cudaEventCreateWithFlags(&c->slotFree[i], cudaEventDisableTiming));
+        RB_CUDA(c, cudaEventCreateWithFlags(&c->slotFull[i], cudaEventDisableTiming));
+    }
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->allocated = true;
+    return rb_reset(c);
+}
+
+rb_status rb_reset(rb_ctx* c) {
+    if (!c) return RB_ERR_INVALID_ARG;
+    if (!c->allocated) return fail(c, RB_ERR_STATE, "reset before allocate");
+    if (c->cfg.pipeline == RB_PIPELINE_FLAT) return RB_OK;
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb::launchResetRoot(c->d, c->numSMs * 2, c->stream);
+    RB_CUDA(c, cudaMemsetAsync(c->d.accumGlobals, 0, sizeof(rb::AccumGlobals), c->stream));
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->batchesConsumed = 0;
+    c->accumAll = true;
+    return RB_OK;
+}
+
+static rb_status buildFrom(rb_ctx* c, const rb::Point* ring, const uint32_t* sizes, uint32_t slots,
+                           uint32_t slotCap, uint32_t numUploaded, uint32_t maxBatches, rb_build_result* out) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const uint32_t first = c->batchesConsumed;
+    const uint32_t avail = numUploaded > first ? numUploaded - first : 0u;
+    const uint32_t nb = std::min(avail, maxBatches);
+    RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
+    k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr);
+    uint32_t done = 0;
+    bool stopped = false;
+    for (uint32_t b = first; b < first + nb; b++) {
+        const uint32_t slot = b % slots;
+        const uint32_t n = sizes[slot];
+        if (n > slotCap) return fail(c, RB_ERR_CAPACITY, "batch larger than its ring slot");
+        rb_status st = runBatch(c, ring + (uint64_t)slot * slotCap, n, b, &stopped);
+        if (st != RB_OK) return st;
+        if (stopped) break;
+        done++;
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (c->cfg.time_budget_ms > 0.0f && ms > c->cfg.time_budget_ms) break;
+    }
+    c->batchesConsumed = first + done;
+    if (c->cfg.accumulate && c->cfg.pipeline == RB_PIPELINE_REMOLOD) {
+        rb_status st = accumulate(c, c->batchesConsumed);
+        if (st != RB_OK) return st;
+    } else if (done > 0) {
+        c->accumAll = true;
+    }
+    RB_CUDA(c, cudaEventRecord(c->evStop, c->stream));
+    RB_CUDA(c, cudaEventSynchronize(c->evStop));
+    if (out) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->evStart, c->evStop);
+        out->batches_consumed = c->batchesConsumed;
+        out->batches_this_call = done;
+        out->mem_capacity_reached = stopped ? 1u : 0u;
+        out->device_ms = ms;
+        out->more = 0;
+    }
+    return RB_OK;
+}
+
+rb_status rb_build(rb_ctx* c, const rb_batch_view* v, rb_build_result* out) {
+    if (!c || !v) return RB_ERR_INVALID_ARG;
+    if (!c->allocated) return fail(c, RB_ERR_STATE, "build before allocate");
+    if (c->cfg.pipeline == RB_PIPELINE_FLAT) return RB_OK;
+    if (out) std::memset(out, 0, sizeof(*out));
+    if (v->slots == 0 || v->batch_sizes == nullptr || v->num_batches_uploaded == 0) return RB_OK;
+    // RemolodPipeline.cpp:315-328: the kernel reads batch B from slot B % ring_slots
+    const uint32_t K = c->cfg.ring_slots;
+    const bool ok = v->num_slots == K || (v->num_batches_total <= K && v->num_slots >= v->num_batches_total);
+    if (!ok)
+        return fail(c, RB_ERR_RING,
+                    "handed a " + std::to_string(v->num_slots) + "-slot ring but batches wrap at " +
+                        std::to_string(K));
+    if (v->slot_capacity != c->cfg.slot_capacity)
+        return fail(c, RB_ERR_RING, "ring slot capacity differs from the configured slot capacity");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    std::vector<uint32_t> sizes(K, 0);
+    for (uint32_t i = 0; i < std::min(K, v->num_slots); i++) sizes[i] = v->batch_sizes[i];
+    rb_status st = buildFrom(c, reinterpret_cast<const rb::Point*>(v->slots), sizes.data(), K,
+                             v->slot_capacity, v->num_batches_uploaded, c->cfg.max_batches_per_build, out);
+    if (st == RB_OK && out) out->more = (v->num_batches_total > 0 && c->batchesConsumed < v->num_batches_total);
+    return st;
+}
+
+rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t batchSize,
+                         rb_build_result* out) {
+    if (!c || (!points && n)) return RB_ERR_INVALID_ARG;
+    if (!c->allocated) return fail(c, RB_ERR_STATE, "ingest before allocate");
+    if (c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_UNSUPPORTED, "flat keeps no tree");
+    if (batchSize == 0 || batchSize > c->cfg.slot_capacity)
+        return fail(c, RB_ERR_CAPACITY, "batch size must be in [1, slot_capacity]");
+    if (out) std::memset(out, 0, sizeof(*out));
+    RB_CUDA(c, cudaSetDevice(c->device));
+    const uint64_t nb = (n + batchSize - 1) / batchSize;
+    const uint32_t S = c->ingestSlots;
+    RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
+    k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr);
+    // the copy stream fills slot (b % S) once the compute stream released it
+    auto issueCopy = [&](uint64_t b) -> rb_status {
+        const uint32_t slot = (uint32_t)(b % S);
+        const uint64_t first = b * batchSize;
+        const uint64_t cnt = std::min<uint64_t>(batchSize, n - first);
+        if (b >= S) RB_CUDA(c, cudaStreamWaitEvent(c->copyStream, c->slotFree[slot], 0));
+        RB_CUDA(c, cudaMemcpyAsync(c->ingestRing + (uint64_t)slot * c->cfg.slot_capacity, points + first,
+                                   cnt * sizeof(rb_point), cudaMemcpyHostToDevice, c->copyStream));
+        RB_CUDA(c, cudaEventRecord(c->slotFull[slot], c->copyStream));
+        return RB_OK;
+    };
+    for (uint64_t b = 0; b < std::min<uint64_t>(nb, S); b++) {
+        rb_status st = issueCopy(b);
+        if (st != RB_OK) return st;
+    }
+    uint32_t done = 0;
+    bool stopped = false;
+    for (uint64_t b = 0; b < nb; b++) {
+        const uint32_t slot = (uint32_t)(b % S);
+        const uint64_t first = b * batchSize;
+        const uint32_t cnt = (uint32_t)std::min<uint64_t>(batchSize, n - first);
+        RB_CUDA(c, cudaStreamWaitEvent(c->stream, c->slotFull[slot], 0));
+        rb_status st = runBatch(c, c->ingestRing + (uint64_t)slot * c->cfg.slot_capacity, cnt,
+                                c->batchesConsumed, &stopped);
+        if (st != RB_OK) return st;
+        RB_CUDA(c, cudaEventRecord(c->slotFree[slot], c->stream));
+        if (stopped) break;
+        c->batchesConsumed++;
+        done++;
+        if (b + S < nb) {
+            st = issueCopy(b + S);
+            if (st != RB_OK) return st;
+        }
+    }
+    if (c->cfg.accumulate && c->cfg.pipeline == RB_PIPELINE_REMOLOD) {
+        rb_status st = accumulate(c, c->batchesConsumed);
+        if (st != RB_OK) return st;
+    } else if (done > 0) {
+        c->accumAll = true;
+    }
+    RB_CUDA(c, cudaEventRecord(c->evStop, c->stream));
+    RB_CUDA(c, cudaEventSynchronize(c->evStop));
+    RB_CUDA(c, cudaStreamSynchronize(c->copyStream));
+    if (out) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->evStart, c->evStop);
+        out->batches_consumed = c->batchesConsumed;
+        out->batches_this_call = done;
+        out->mem_capacity_reached = stopped ? 1u : 0u;
+        out->device_ms = ms;
+    }
+    return RB_OK;
+}
+
+rb_status rb_accumulate(rb_ctx* c, uint32_t batchIndex, rb_accum_globals* out) {
+    if (!c) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = accumulate(c, batchIndex);
+    if (st != RB_OK) return st;
+    if (out) {
+        RB_CUDA(c, cudaMemcpyAsync(c->hostAccum, c->d.accumGlobals, sizeof(rb::AccumGlobals),
+                                   cudaMemcpyDeviceToHost, c->stream));
+        RB_CUDA(c, cudaStreamSynchronize(c->stream));
+        static_assert(sizeof(rb_accum_globals) == sizeof(rb::AccumGlobals), "AccumGlobals layout");
+        std::memcpy(out, c->hostAccum, sizeof(*out));
+    }
+    return RB_OK;
+}
+
+static rb::Frame toFrame(const rb_frame* f) {
+    rb::Frame r;
+    r.width = f->width;
+    r.height = f->height;
+    std::memcpy(r.transform, f->transform, sizeof(r.transform));
+    std::memcpy(r.transformFrozen, f->transform_frozen, sizeof(r.transformFrozen));
+    for (int a = 0; a < 3; a++) {
+        r.boxMin[a] = f->box_min[a];
+        r.boxMax[a] = f->box_max[a];
+    }
+    r.lodPixelBudget = f->lod_pixel_budget;
+    r.pointSize = f->point_size;
+    return r;
+}
+
+static rb_status finishFrame(rb_ctx* c, const rb_frame* f, unsigned long long* fb, uint32_t* rgba,
+                             uint64_t npx) {
+    if (f->enable_edl) {
+        if (c->fbTmpPixels < npx) {
+            if (c->fbTmp) cudaFree(c->fbTmp);
+            c->fbTmp = nullptr;
+            c->fbTmpPixels = 0;
+            RB_CUDA(c, cudaMalloc(&c->fbTmp, npx * 8));
+            c->fbTmpPixels = npx;
+        }
+        RB_CUDA(c, cudaMemcpyAsync(c->fbTmp, fb, npx * 8, cudaMemcpyDeviceToDevice, c->stream));
+        rb::launchEdl(c->fbTmp, fb, (uint32_t)f->width, (uint32_t)f->height, f->edl_strength,
+                      c->numSMs * 8, c->stream);
+    }
+    if (rgba) rb::launchResolve(fb, rgba, npx, c->numSMs * 8, c->stream);
+    return RB_OK;
+}
+
+rb_status rb_render(rb_ctx* c, const rb_frame* f, uint64_t fbDev, uint64_t rgbaDev, uint64_t forceDev,
+                    rb_render_result* out) {
+    if (!c || !f || !fbDev) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree to render");
+    if (!(f->width >= 1.0f && f->height >= 1.0f)) return fail(c, RB_ERR_INVALID_ARG, "empty frame");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    const uint64_t npx = (uint64_t)f->width * (uint64_t)f->height;
+    auto* fb = reinterpret_cast<unsigned long long*>(fbDev);
+    const rb::Frame fr = toFrame(f);
+    const uint32_t cap = std::max<uint32_t>(c->cfg.drawlist_capacity, 1);
+    RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
+    rb::launchFbClear(fb, npx, c->numSMs * 8, c->stream);
+    rb::launchNodeFlags(c->d, fr, c->vis, c->large, reinterpret_cast<const uint8_t*>(forceDev), c->rs,
+                        c->numSMs * 4, c->stream);
+    rb::launchFrontier(c->d, c->vis, c->large, c->rs, c->items, cap, c->numSMs * 4, c->stream);
+    rb::launchRaster(c->d, fr, fb, c->rs, c->items, cap, c->numSMs * 8, c->stream);
+    rb_status st = finishFrame(c, f, fb, reinterpret_cast<uint32_t*>(rgbaDev), npx);
+    if (st != RB_OK) return st;
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaEventRecord(c->evStop, c->stream));
+    RB_CUDA(c, cudaMemcpyAsync(c->hostRs, c->rs, sizeof(rb::RenderScratch), cudaMemcpyDeviceToHost, c->stream));
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->lastVisibleNodes = c->hostRs->numItems;
+    c->lastVisibleSamples = c->hostRs->samples;
+    if (out) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->evStart, c->evStop);
+        out->draw_items = c->hostRs->numItems;
+        out->drawlist_overflow = c->hostRs->overflow;
+        out->draw_samples = c->hostRs->samples;
+        out->device_ms = ms;
+    }
+    return RB_OK;
+}
+
+rb_status rb_render_flat(rb_ctx* c, const rb_frame* f, uint64_t pointsDev, uint64_t n, uint64_t fbDev,
+                         uint64_t rgbaDev, rb_render_result* out) {
+    if (!c || !f || !fbDev || (!pointsDev && n)) return RB_ERR_INVALID_ARG;
+    if (!c->allocated) return fail(c, RB_ERR_STATE, "render before allocate");
+    if (!(f->width >= 1.0f && f->height >= 1.0f)) return fail(c, RB_ERR_INVALID_ARG, "empty frame");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    const uint64_t npx = (uint64_t)f->width * (uint64_t)f->height;
+    auto* fb = reinterpret_cast<unsigned long long*>(fbDev);
+    const rb::Frame fr = toFrame(f);
+    RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
+    rb::launchFbClear(fb, npx, c->numSMs * 8, c->stream);
+    if (n) rb::launchRasterFlat(fr, fb, reinterpret_cast<const rb::Point*>(pointsDev), n, c->numSMs * 16, c->stream);
+    rb_status st = finishFrame(c, f, fb, reinterpret_cast<uint32_t*>(rgbaDev), npx);
+    if (st != RB_OK) return st;
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaEventRecord(c->evStop, c->stream));
+    RB_CUDA(c, cudaEventSynchronize(c->evStop));
+    if (out) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->evStart, c->evStop);
+        out->draw_items = (uint32_t)((n + 65535) / 65536);  // the reference's 64K slices
+        out->drawlist_overflow = 0;
+        out->draw_samples = n;
+        out->device_ms = ms;
+    }
+    return RB_OK;
+}
+
+rb_status rb_read_stats(rb_ctx* c, rb_stats* o) {
+    if (!c || !o) return RB_ERR_INVALID_ARG;
+    std::memset(o, 0, sizeof(*o));
+    if (!c->allocated) return fail(c, RB_ERR_STATE, "stats before allocate");
+    o->bytes_allocated = c->bytes;
+    if (c->cfg.pipeline == RB_PIPELINE_FLAT) return RB_OK;
+    RB_CUDA(c, cudaSetDevice(c->device));
+    RB_CUDA(c, cudaMemsetAsync(c->d.sweep, 0, sizeof(rb::SweepStats), c->stream));
+    rb::launchSweep(c->d, c->numSMs * 4, c->stream);
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaMemcpyAsync(c->hostSweep, c->d.sweep, sizeof(rb::SweepStats), cudaMemcpyDeviceToHost, c->stream));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    const Counters& k = *c->hostCtr;
+    const rb::SweepStats& s = *c->hostSweep;
+    o->num_points = s.numPoints;
+    o->num_voxels = s.numVoxels;
+    o->num_points_ingested = k.numPointsProcessed;
+    o->num_nodes = k.numNodes;
+    o->num_inner = s.numInner;
+    o->num_leaves = s.numLeaves;
+    o->num_nonempty_leaves = s.numNonemptyLeaves;
+    o->max_depth = s.maxLevel;
+    o->max_points_per_node = s.maxPointsPerNode;
+    o->num_chunks_points = s.numChunksPoints;
+    o->num_chunks_voxels = s.numChunksVoxels;
+    o->batchlet_index = k.batchletIndex;
+    o->counter_underflows = s.counterUnderflows;
+    o->num_allocated_chunks = k.numAllocatedChunks;
+    o->chunk_pool_size = k.chunkPoolSize;
+    o->persistent_offset = k.refOffset;
+    o->persistent_capacity = c->d.persistentCapacity;
+    o->dropped_points = k.droppedPoints;
+    o->expand_iters = k.expandIters;
+    o->nodes_split = k.nodesSplit;
+    o->spilled_points = k.spilledPointsTotal;
+    o->num_grids = k.numGrids;
+    o->overflow_flags = k.overflowFlags;
+    o->mem_capacity_reached = k.memCapacityReached;
+    o->node_capacity_reached = k.nodePoolOverflow || k.numNodes >= c->cfg.max_nodes;
+    o->num_visible_nodes = c->lastVisibleNodes;
+    o->num_visible_samples = c->lastVisibleSamples;
+    return RB_OK;
+}
+
+rb_status rb_read_nodes(rb_ctx* c, rb_node_info* out, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    const uint32_t nn = c->hostCtr->numNodes;
+    *count = nn;
+    if (!out) return RB_OK;
+    if (capacity < nn) return fail(c, RB_ERR_CAPACITY, "node buffer too small");
+    std::vector<int32_t> child((size_t)nn * 8);
+    std::vector<uint32_t> a[10];
+    uint32_t* src[10] = {c->d.counter, c->d.numPoints, c->d.level, c->d.nodeX, c->d.nodeY, c->d.nodeZ,
+                         c->d.grid, c->d.numVoxels, c->d.numPointChunks, c->d.numVoxelChunks};
+    RB_CUDA(c, cudaMemcpy(child.data(), c->d.child, (size_t)nn * 32, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 10; k++) {
+        a[k].resize(nn);
+        RB_CUDA(c, cudaMemcpy(a[k].data(), src[k], (size_t)nn * 4, cudaMemcpyDeviceToHost));
+    }
+    for (uint32_t i = 0; i < nn; i++) {
+        rb_node_info& o = out[i];
+        bool leaf = true;
+        for (int q = 0; q < 8; q++) {
+            o.child[q] = child[(size_t)i * 8 + q];
+            if (o.child[q] >= 0) leaf = false;
+        }
+        o.counter = a[0][i];
+        o.num_points = a[1][i];
+        o.level = a[2][i];
+        o.X = a[3][i];
+        o.Y = a[4][i];
+        o.Z = a[5][i];
+        o.has_grid = a[6][i] != kNone;
+        o.num_voxels = a[7][i];
+        o.num_point_chunks = a[8][i];
+        o.num_voxel_chunks = a[9][i];
+        o.is_leaf = leaf;
+    }
+    return RB_OK;
+}
+
+static rb_status readChunked(rb_ctx* c, uint32_t node, bool voxels, rb_point* pts, uint32_t* idx,
+                             uint32_t capacity, uint32_t* count) {
+    RB_CUDA(c, cudaSetDevice(c->device));
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    if (node >= c->hostCtr->numNodes) return fail(c, RB_ERR_INVALID_ARG, "node out of range");
+    uint32_t n = 0, nch = 0, off = 0, stored = 0;
+    RB_CUDA(c, cudaMemcpy(&n, (voxels ? c->d.numVoxels : c->d.numPoints) + node, 4, cudaMemcpyDeviceToHost));
+    RB_CUDA(c, cudaMemcpy(&nch, (voxels ? c->d.numVoxelChunks : c->d.numPointChunks) + node, 4,
+                          cudaMemcpyDeviceToHost));
+    RB_CUDA(c, cudaMemcpy(&off, (voxels ? c->d.vxTableOff : c->d.ptTableOff) + node, 4, cudaMemcpyDeviceToHost));
+    if (voxels) {
+        RB_CUDA(c, cudaMemcpy(&stored, c->d.numVoxelsStored + node, 4, cudaMemcpyDeviceToHost));
+        n = std::min(n, stored);
+    }
+    const uint32_t ppc = c->d.ppc;
+    n = std::min<uint32_t>(n, nch * ppc);
+    *count = n;
+    if (!pts) return RB_OK;
+    if (capacity < n) return fail(c, RB_ERR_CAPACITY, "point buffer too small");
+    if (n == 0) return RB_OK;
+    std::vector<uint32_t> table(nch);
+    RB_CUDA(c, cudaMemcpy(table.data(), c->d.tablePool + off, (size_t)nch * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t j = 0; j * ppc < n; j++) {
+        const uint32_t cnt = std::min(ppc, n - j * ppc);
+        if (table[j] == kNone) return fail(c, RB_ERR_STATE, "chunk missing");
+        const uint8_t* base = c->d.arena + (uint64_t)table[j] * 16ull;
+        RB_CUDA(c, cudaMemcpy(pts + (size_t)j * ppc, base, (size_t)cnt * 16, cudaMemcpyDeviceToHost));
+        if (idx && !voxels)
+            RB_CUDA(c, cudaMemcpy(idx + (size_t)j * ppc, base + (uint64_t)ppc * 16, (size_t)cnt * 4,
+                                  cudaMemcpyDeviceToHost));
+    }
+    return RB_OK;
+}
+
+rb_status rb_read_node_points(rb_ctx* c, uint32_t node, rb_point* pts, uint32_t* idx, uint32_t capacity,
+                              uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
+    return readChunked(c, node, false, pts, idx, capacity, count);
+}
+
+rb_status rb_read_node_voxels(rb_ctx* c, uint32_t node, rb_point* vox, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
+    return readChunked(c, node, true, vox, nullptr, capacity, count);
+}
+
+rb_status rb_read_node_grid(rb_ctx* c, uint32_t node, uint32_t* words) {
+    if (!c || !words) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    if (node >= c->hostCtr->numNodes) return fail(c, RB_ERR_INVALID_ARG, "node out of range");
+    uint32_t g = kNone;
+    RB_CUDA(c, cudaMemcpy(&g, c->d.grid + node, 4, cudaMemcpyDeviceToHost));
+    if (g == kNone) return fail(c, RB_ERR_INVALID_ARG, "node has no grid");
+    RB_CUDA(c, cudaMemcpy(words, c->d.arena + (uint64_t)g * 16ull, rb::kGridBytes, cudaMemcpyDeviceToHost));
+    return RB_OK;
+}
+
+rb_status rb_read_accums(rb_ctx* c, rb_accum* out, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
+    static_assert(sizeof(rb_accum) == sizeof(rb::AccumI), "accumulator layout");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    const uint32_t nn = c->hostCtr->numNodes;
+    *count = nn;
+    if (!out) return RB_OK;
+    if (capacity < nn) return fail(c, RB_ERR_CAPACITY, "accumulator buffer too small");
+    RB_CUDA(c, cudaMemcpy(out, c->d.accum, (size_t)nn * sizeof(rb_accum), cudaMemcpyDeviceToHost));
+    return RB_OK;
+}
+
+}  // extern "C"

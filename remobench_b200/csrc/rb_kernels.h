@@ -1,0 +1,62 @@
+// Kernel launch wrappers shared by the stage translation units and the host
+// orchestration (rb_capi.cu). Host code never sees a kernel symbol directly.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rb_state.h"
+
+namespace rb {
+
+// Per-frame render parameters (the subset of SharedUniforms,
+// include/remo/HostDeviceCommon.h:28-60, that the LOD cut and splat read).
+struct Frame {
+    float width, height;
+    float transform[16];        // row-major, clip = M (x, y, z, 1)
+    float transformFrozen[16];  // LOD-selection and frustum transform
+    float boxMin[3], boxMax[3];
+    float lodPixelBudget;
+    int32_t pointSize;
+};
+
+struct RenderScratch {
+    uint32_t numItems;
+    uint32_t overflow;
+    unsigned long long samples;
+};
+
+// Update
+void launchBatchBegin(const Dev& d, cudaStream_t s);
+void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
+void launchRecount(const Dev& d, const Point* pts, uint32_t n, uint32_t prevStamp, int grid, cudaStream_t s);
+void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s);
+void launchSpillCopy(const Dev& d, int grid, cudaStream_t s);
+void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
+void launchVoxCommit(const Dev& d, int grid, cudaStream_t s);
+void launchAllocChunks(const Dev& d, int grid, cudaStream_t s);
+void launchInsert(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
+void launchVoxStore(const Dev& d, int grid, cudaStream_t s);
+void launchBatchEnd(const Dev& d, uint32_t n, cudaStream_t s);
+void launchSweep(const Dev& d, int grid, cudaStream_t s);
+void launchResetRoot(const Dev& d, int grid, cudaStream_t s);
+
+// Accumulate
+void launchAccumulate(const Dev& d, uint32_t batchIndex, int useList, int grid, cudaStream_t s);
+void launchAccumVerify(const Dev& d, int grid, cudaStream_t s);
+
+// Rasterize
+void launchFbClear(unsigned long long* fb, uint64_t npx, int grid, cudaStream_t s);
+void launchNodeFlags(const Dev& d, const Frame& f, uint8_t* vis, uint8_t* large, const uint8_t* force,
+                     RenderScratch* rs, int grid, cudaStream_t s);
+void launchFrontier(const Dev& d, const uint8_t* vis, const uint8_t* large, RenderScratch* rs,
+                    uint32_t* items, uint32_t cap, int grid, cudaStream_t s);
+void launchRaster(const Dev& d, const Frame& f, unsigned long long* fb, const RenderScratch* rs,
+                  const uint32_t* items, uint32_t cap, int grid, cudaStream_t s);
+void launchRasterFlat(const Frame& f, unsigned long long* fb, const Point* pts, uint64_t n, int grid,
+                      cudaStream_t s);
+void launchEdl(const unsigned long long* src, unsigned long long* dst, uint32_t w, uint32_t h,
+               float strength, int grid, cudaStream_t s);
+void launchResolve(const unsigned long long* fb, uint32_t* rgba, uint64_t npx, int grid, cudaStream_t s);
+
+}  // namespace rb

@@ -1,0 +1,213 @@
+// Device-side state of one LOD context: the node pool as structure-of-arrays,
+// the chunk and grid pools, per-batch scratch and the counter block. Shared by
+// every kernel translation unit and by the host orchestration in rb_capi.cu.
+//
+// Data model (restates kernels/remolod/remolod_structures.cuh:12-135 for the
+// B200): nodes are integer ids into flat arrays, not pointers; a node's 8
+// children are one 32-byte row of `child`, so a descent step is one sector
+// load; a leaf's points live in 1000-point chunks reached through a per-node
+// chunk table instead of a linked list, so slot s is table[s / 1000] with no
+// walk (the reference walks the list from its head for every point,
+// remolod_octree.cu:853-857).
+#pragma once
+
+#include <stdint.h>
+
+namespace rb {
+
+constexpr int kMaxDepth = 20;                 // remolod_structures.cuh:18
+constexpr uint32_t kGridSize = 128;           // :16
+constexpr uint32_t kGridWords = 65536;        // 128^3 bits as 32-bit words (:66-68)
+constexpr uint64_t kGridBytes = 262144ull;
+constexpr uint64_t kRefChunkBytes = 16016ull; // sizeof(Chunk) in the reference (:59-64)
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint64_t kHashEmpty = ~0ull;
+
+// AllocatorGlobal::alloc's rounding (kernels/simlod/utils.h.cu:195)
+__host__ __device__ inline uint64_t refAllocSize(uint64_t size) {
+    return 16ull * ((size + 16ull) / 16ull);
+}
+
+struct Point {
+    float x, y, z;
+    uint32_t color;
+};
+
+// Counter block, one per context, in device memory.
+struct Counters {
+    uint32_t numNodes;
+    uint32_t arenaBump;         // arena units (16 B) handed out
+    uint32_t numGrids;          // grids handed out
+    uint32_t numPtChunks;       // point chunks ever taken from the arena
+    uint32_t numVxChunks;       // voxel chunks ever taken from the arena
+    uint32_t tableBump;         // chunk-table entries handed out
+    uint32_t numAllocatedChunks;  // Stats::numAllocatedChunks (logical queue length)
+    uint32_t chunkPoolSize;       // Stats::chunkPoolSize
+    uint32_t batchletIndex;       // Stats::batchletIndex
+    uint64_t numPointsProcessed;  // Stats::numPointsProcessed
+    uint64_t refOffset;           // the reference store's AllocatorGlobal::offset
+    // per batch
+    uint32_t batchStop;           // memCapacityReached for this batch
+    uint32_t iter;                // expand iteration being counted (1-based)
+    uint32_t numSpill;            // spilling nodes found by the last count
+    uint32_t numSplit;            // nodes split by the last split
+    uint32_t numSpilled;          // spilled points this batch
+    uint32_t numNew;              // new voxel cells this batch
+    uint32_t spillChunkTotal;     // copy work items of the last split
+    uint32_t pad0;
+    // flags and diagnostics (sticky until reset)
+    uint32_t memCapacityReached;
+    uint32_t nodePoolOverflow;
+    uint32_t overflowFlags;       // RB_OVF_* bits
+    uint32_t pad1;
+    uint64_t droppedPoints;
+    uint64_t expandIters;
+    uint64_t nodesSplit;
+    uint64_t spilledPointsTotal;
+    // dirty list for Accumulate
+    uint32_t numDirty;
+    uint32_t buildStamp;
+    uint32_t pad2;
+};
+
+enum OverflowBits : uint32_t {
+    kOvfSpilled = 1u,     // spill list full
+    kOvfBacklog = 2u,     // voxel hash full or probe limit
+    kOvfSpilling = 4u,    // spilling-node list full
+    kOvfArena = 8u,       // arena full (grids and chunks)
+    kOvfTables = 64u,     // chunk-table pool full
+    kOvfDirty = 128u,     // dirty list full
+    kOvfDrawList = 256u,  // render draw list full
+};
+
+// One node split by the last split pass: where its stored points go.
+struct SplitRec {
+    uint32_t node;
+    uint32_t numPoints;     // points stored before the split
+    uint32_t tableOff;      // its point chunk table (kept readable for the copy)
+    uint32_t spillBase;     // first spill slot of its points
+    uint32_t chunkBase;     // first copy work item
+    uint32_t numChunks;
+    uint32_t grid;
+    uint32_t pad;
+};
+
+// Exact integer sums of one node (see rb_accum.cu).
+struct AccumI {
+    unsigned long long s1[3];
+    unsigned long long s2lo[6];
+    unsigned long long s2hi[6];
+    unsigned long long c1[3];
+    unsigned long long c2[3];
+    uint32_t count;
+    uint32_t lastTouchedBatch;
+    uint32_t state;
+    uint32_t pad;
+};
+
+struct AccumGlobals {
+    unsigned long long mortonWatermark;
+    unsigned long long numAccumulated;
+    unsigned long long sumLeafCounts;
+    uint32_t pointsFolded;
+    uint32_t numLeavesFolded;
+    uint32_t innerWithSums;
+    uint32_t pad;
+};
+
+// Stats sweep output (remolod_octree.cu:1271-1310).
+struct SweepStats {
+    uint32_t numInner, numLeaves, numNonemptyLeaves, maxPointsPerNode;
+    unsigned long long numPoints, numVoxels;
+    uint32_t numChunksPoints, numChunksVoxels, counterUnderflows, maxLevel;
+};
+
+// Everything a kernel needs, passed by value.
+struct Dev {
+    // node pool
+    int32_t* child;          // [maxNodes * 8], -1: none
+    uint32_t* counter;
+    uint32_t* numPoints;
+    uint32_t* level;
+    uint32_t* nodeX;
+    uint32_t* nodeY;
+    uint32_t* nodeZ;
+    uint32_t* grid;          // arena unit offset of the node's occupancy grid, kNone: none
+    uint32_t* numVoxels;
+    uint32_t* numVoxelsStored;
+    uint32_t* numPointChunks;
+    uint32_t* numVoxelChunks;
+    uint32_t* ptTableOff;
+    uint32_t* ptTableCap;
+    uint32_t* vxTableOff;
+    uint32_t* vxTableCap;
+    uint32_t* splitIter;     // 1-based expand iteration of the split in this batch, 0: none
+    uint32_t* dirtyStamp;
+    AccumI* accum;
+    // storage: one arena in 16-byte units holding grids (256 KB), point chunks
+    // (ppc points, then ppc global point indices) and voxel chunks (ppc voxels);
+    // chunk tables and grid ids hold arena unit offsets
+    uint8_t* arena;
+    uint32_t* tablePool;
+    uint32_t* chunkQueue;    // [maxPtChunks] recycled chunk ids (remolod_octree.cu:349-360)
+    // per-batch scratch
+    uint32_t* leafOf;        // [slotCapacity]
+    Point* spillPts;         // [spillCap]
+    uint32_t* spillIdx;
+    uint32_t* spillLeaf;
+    uint32_t* spillNodes;    // [spillingCap] nodes whose counter crossed the limit
+    SplitRec* splitRecs;     // [spillingCap]
+    unsigned long long* hashKeys;  // [hashMask + 1]
+    unsigned long long* hashVals;
+    uint32_t* hashNew;       // [newCap] slots inserted this batch
+    uint32_t* hashNewNode;   // node of each new cell
+    uint32_t* hashNewSlot;   // slot of the new voxel within its node
+    uint32_t* dirtyList;     // [maxNodes]
+    Counters* ctr;
+    SweepStats* sweep;
+    AccumGlobals* accumGlobals;
+    // capacities and constants
+    uint32_t maxNodes;
+    uint32_t maxPointsPerNode;
+    uint32_t ppc;            // points per chunk
+    uint32_t maxPtChunks;    // chunk queue capacity
+    uint32_t arenaUnits;
+    uint32_t ptChunkUnits;
+    uint32_t vxChunkUnits;
+    uint32_t tablePoolCap;
+    uint32_t spillCap;
+    uint32_t spillingCap;
+    uint32_t hashMask;
+    uint32_t newCap;
+    uint32_t maxExpandIters;
+    uint32_t voxelMode;      // 0: lowest index wins, 1: first to arrive
+    uint64_t persistentCapacity;  // the reference store's capacity (bytes)
+    uint64_t safetyMargin;
+    float boxMin[3];
+    float octreeSize;
+};
+
+constexpr uint32_t kGridUnits = (uint32_t)(kGridBytes / 16u);
+
+#ifdef __CUDACC__
+__device__ __forceinline__ Point* chunkPoints(const Dev& d, uint32_t phys) {
+    return reinterpret_cast<Point*>(d.arena + (uint64_t)phys * 16u);
+}
+__device__ __forceinline__ uint32_t* chunkIndices(const Dev& d, uint32_t phys) {
+    return reinterpret_cast<uint32_t*>(d.arena + (uint64_t)phys * 16u + (uint64_t)d.ppc * 16u);
+}
+__device__ __forceinline__ uint32_t* gridWordsAt(const Dev& d, uint32_t g) {
+    return reinterpret_cast<uint32_t*>(d.arena + (uint64_t)g * 16u);
+}
+// Bump allocation of `units` 16-byte units; kNone when the arena is full.
+__device__ __forceinline__ uint32_t arenaAlloc(const Dev& d, uint32_t units) {
+    const uint32_t off = atomicAdd(&d.ctr->arenaBump, units);
+    if ((uint64_t)off + units > d.arenaUnits) {
+        atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfArena);
+        return kNone;
+    }
+    return off;
+}
+#endif
+
+}  // namespace rb

@@ -1,0 +1,762 @@
+// Update stage: count -> split -> make room -> 128^3 voxel sampling -> chunk
+// acquisition -> point and voxel insertion, one batch at a time.
+//
+// Restates kernels/remolod/remolod_octree.cu:95-1060 (addBatch and its phases)
+// as phase kernels on one stream. Every kernel here is plain SIMT integer work
+// bound by latency and L2 atomics, not by tensor cores; see the per-kernel
+// notes for what each reads and writes.
+//
+// Parity-critical float arithmetic (quantisation, voxel centres) uses the
+// explicitly rounded intrinsics (__fsub_rn, __fmul_rn, __fdiv_rn, __fmaf_rn),
+// so nvcc cannot contract or approximate it; the CPU oracle performs the same
+// operations in the same order.
+#include <cuda_runtime.h>
+
+#include "rb_kernels.h"
+#include "rb_state.h"
+
+namespace rb {
+
+__device__ __forceinline__ uint32_t quant20(float c, float mn, float size) {
+    float d = __fsub_rn(c, mn);
+    return __float2uint_rz(__fdiv_rn(__fmul_rn(1048576.0f, d), size));
+}
+
+__device__ __forceinline__ uint32_t quant28(float c, float mn, float size) {
+    float d = __fsub_rn(c, mn);
+    return __float2uint_rz(__fdiv_rn(__fmul_rn(268435456.0f, d), size));
+}
+
+__device__ __forceinline__ Point loadPoint(const Point* p) {
+    float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    Point q;
+    q.x = v.x;
+    q.y = v.y;
+    q.z = v.z;
+    q.color = __float_as_uint(v.w);
+    return q;
+}
+
+__device__ __forceinline__ uint32_t childIndex(uint32_t x, uint32_t y, uint32_t z, uint32_t level) {
+    const uint32_t s = kMaxDepth - level - 1;
+    return (((x >> s) & 1u) << 2) | (((y >> s) & 1u) << 1) | ((z >> s) & 1u);
+}
+
+// remolod_octree.cu:182-201: at most kMaxDepth steps from the root.
+__device__ __forceinline__ uint32_t descendFromRoot(const Dev& d, uint32_t x, uint32_t y, uint32_t z) {
+    uint32_t cur = 0;
+    for (uint32_t level = 0; level < (uint32_t)kMaxDepth; level++) {
+        int32_t c = __ldg(&d.child[cur * 8u + childIndex(x, y, z, level)]);
+        if (c < 0) break;
+        cur = (uint32_t)c;
+    }
+    return cur;
+}
+
+__device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
+
+// Warp-aggregated count at a leaf (remolod_octree.cu:203-220). Every lane of
+// the warp must call it; lanes with nothing to count pass kNone.
+__device__ __forceinline__ void countAt(const Dev& d, uint32_t leaf) {
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, leaf);
+    if (leaf == kNone) return;
+    if ((int)laneId() != __ffs(peers) - 1) return;
+    const uint32_t g = __popc(peers);
+    const uint32_t old = atomicAdd(&d.counter[leaf], g);
+    if (old <= d.maxPointsPerNode && old + g > d.maxPointsPerNode) {
+        const uint32_t k = atomicAdd(&d.ctr->numSpill, 1u);
+        if (k < d.spillingCap) d.spillNodes[k] = leaf;
+        else atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfSpilling);
+    }
+}
+
+__global__ void k_batch_begin(Dev d) {
+    Counters* c = d.ctr;
+    const bool stop = c->refOffset + d.safetyMargin >= d.persistentCapacity;
+    c->batchStop = stop ? 1u : 0u;
+    c->memCapacityReached = stop ? 1u : 0u;
+    c->numSpill = 0;
+    c->numSpilled = 0;
+    c->numNew = 0;
+    c->numSplit = 0;
+    c->spillChunkTotal = 0;
+    c->iter = 1;
+}
+
+// Iteration 1 of expand (doCounting over the batch, remolod_octree.cu:225-229):
+// descend every batch point, remember its leaf, count it there.
+__global__ void __launch_bounds__(256) k_count_first(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    if (d.ctr->batchStop) return;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t leaf = kNone;
+        if (i < n) {
+            const Point p = loadPoint(pts + i);
+            leaf = descendFromRoot(d, quant20(p.x, d.boxMin[0], d.octreeSize),
+                                   quant20(p.y, d.boxMin[1], d.octreeSize),
+                                   quant20(p.z, d.boxMin[2], d.octreeSize));
+            d.leafOf[i] = leaf;
+        }
+        countAt(d, leaf);
+    }
+}
+
+// Iterations 2.. of expand. The reference re-descends every batch and spilled
+// point from the root and counts only at leaves created by the last split
+// (countIteration, remolod_octree.cu:203). A point can only reach such a leaf
+// if its own leaf was split, so only those points move, one level, from the
+// leaf they were in; the counts that result are the same.
+__device__ __forceinline__ uint32_t stepIfSplit(const Dev& d, uint32_t cur, const Point& p,
+                                                uint32_t prevStamp) {
+    if (d.splitIter[cur] != prevStamp) return kNone;
+    const uint32_t lv = d.level[cur];
+    if (lv >= (uint32_t)kMaxDepth) return kNone;
+    const uint32_t ci = childIndex(quant20(p.x, d.boxMin[0], d.octreeSize),
+                                   quant20(p.y, d.boxMin[1], d.octreeSize),
+                                   quant20(p.z, d.boxMin[2], d.octreeSize), lv);
+    return (uint32_t)d.child[cur * 8u + ci];
+}
+
+__global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict__ pts, uint32_t n,
+                                                 uint32_t prevStamp) {
+    if (d.ctr->batchStop) return;
+    const uint32_t ns = d.ctr->numSpilled < d.spillCap ? d.ctr->numSpilled : d.spillCap;
+    const uint32_t total = n + ns;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t leaf = kNone;
+        if (i < n) {
+            const uint32_t cur = d.leafOf[i];
+            if (d.splitIter[cur] == prevStamp) {
+                leaf = stepIfSplit(d, cur, loadPoint(pts + i), prevStamp);
+                if (leaf != kNone) d.leafOf[i] = leaf;
+            }
+        } else if (i < total) {
+            const uint32_t j = i - n;
+            const uint32_t cur = d.spillLeaf[j];
+            if (d.splitIter[cur] == prevStamp) {
+                leaf = stepIfSplit(d, cur, d.spillPts[j], prevStamp);
+                if (leaf != kNone) d.spillLeaf[j] = leaf;
+            }
+        }
+        countAt(d, leaf);
+    }
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x == 1024).
+__device__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* total, uint32_t* s_warp) {
+    const uint32_t lane = laneId(), warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < (blockDim.x >> 5) ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        s_warp[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t prefix = (warp > 0 ? s_warp[warp - 1] : 0u) + x - v;
+    *total = s_warp[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return prefix;
+}
+
+// Ascending bitonic sort of n ids in place (single block); pads with kNone.
+__device__ void bitonicSort(uint32_t* a, uint32_t n) {
+    uint32_t m = 1;
+    while (m < n) m <<= 1;
+    for (uint32_t i = n + threadIdx.x; i < m; i += blockDim.x) a[i] = kNone;
+    __syncthreads();
+    for (uint32_t k = 2; k <= m; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const uint32_t ai = a[i], al = a[l];
+                    const bool up = (i & k) == 0;
+                    if ((ai > al) == up) {
+                        a[i] = al;
+                        a[l] = ai;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+constexpr uint32_t kSortSmem = 8192;
+
+// doSplitting (remolod_octree.cu:303-400) for the nodes the last count found,
+// in increasing node id, each taking the next block of 8 ids. One block of
+// 1024 threads: the list is short (14 nodes per batch on the reference's
+// 36M cloud, wiki/03_ExpandStageFindings.md:63).
+__global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
+    __shared__ uint32_t s_sort[kSortSmem];
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_runPts, s_runChunks;
+    Counters* c = d.ctr;
+    if (c->batchStop) return;
+    uint32_t ns = c->numSpill;
+    if (ns > d.spillingCap) ns = d.spillingCap;
+    if (ns == 0) {
+        if (threadIdx.x == 0) c->numSplit = 0;
+        return;
+    }
+    uint32_t* list;
+    if (ns <= kSortSmem) {
+        for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s_sort[i] = d.spillNodes[i];
+        __syncthreads();
+        bitonicSort(s_sort, ns);
+        list = s_sort;
+    } else {
+        // rare: sorts in the spilling-node buffer itself (sized to a power of two)
+        bitonicSort(d.spillNodes, ns);
+        list = d.spillNodes;
+    }
+    const uint32_t nn = c->numNodes;
+    const uint32_t room = d.maxNodes > nn ? (d.maxNodes - nn) / 8u : 0u;
+    const uint32_t acc = ns < room ? ns : room;
+    const uint32_t spilledBefore = c->numSpilled;
+    if (threadIdx.x == 0) {
+        if (acc < ns) c->nodePoolOverflow = 1;
+        s_runPts = 0;
+        s_runChunks = 0;
+    }
+    __syncthreads();
+    for (uint32_t k0 = 0; k0 < acc; k0 += blockDim.x) {
+        const uint32_t k = k0 + threadIdx.x;
+        uint32_t node = 0, np = 0, nch = 0;
+        if (k < acc) {
+            node = list[k];
+            const uint32_t cap = d.numPointChunks[node] * d.ppc;
+            np = d.numPoints[node] < cap ? d.numPoints[node] : cap;
+            nch = (np + d.ppc - 1) / d.ppc;
+        }
+        uint32_t totPts, totCh;
+        const uint32_t prePts = blockExclusiveScan(np, &totPts, s_warp);
+        const uint32_t preCh = blockExclusiveScan(nch, &totCh, s_warp);
+        if (k < acc) {
+            const uint32_t base = nn + 8u * k;
+            const uint32_t lv = d.level[node] + 1u;
+            const uint32_t X = d.nodeX[node], Y = d.nodeY[node], Z = d.nodeZ[node];
+            for (uint32_t i = 0; i < 8; i++) {
+                const uint32_t ch = base + i;
+#pragma unroll
+                for (int q = 0; q < 8; q++) d.child[ch * 8u + q] = -1;
+                d.counter[ch] = 0;
+                d.numPoints[ch] = 0;
+                d.level[ch] = lv;
+                d.nodeX[ch] = 2u * X + ((i >> 2) & 1u);
+                d.nodeY[ch] = 2u * Y + ((i >> 1) & 1u);
+                d.nodeZ[ch] = 2u * Z + (i & 1u);
+                d.grid[ch] = kNone;
+                d.numVoxels[ch] = 0;
+                d.numVoxelsStored[ch] = 0;
+                d.numPointChunks[ch] = 0;
+                d.numVoxelChunks[ch] = 0;
+                d.ptTableOff[ch] = kNone;
+                d.ptTableCap[ch] = 0;
+                d.vxTableOff[ch] = kNone;
+                d.vxTableCap[ch] = 0;
+                d.splitIter[ch] = 0;
+                d.dirtyStamp[ch] = 0;
+                AccumI z = {};
+                d.accum[ch] = z;
+                d.child[node * 8u + i] = (int32_t)ch;
+            }
+            d.splitIter[node] = stamp;
+            SplitRec r;
+            r.node = node;
+            r.numPoints = np;
+            r.tableOff = d.ptTableOff[node];
+            r.spillBase = spilledBefore + s_runPts + prePts;
+            r.chunkBase = s_runChunks + preCh;
+            r.numChunks = nch;
+            // chunks go back to the queue (remolod_octree.cu:349-360)
+            const uint32_t owned = d.numPointChunks[node];
+            for (uint32_t j = 0; j < owned; j++) {
+                const uint32_t idx = atomicSub(&c->numAllocatedChunks, 1u) - 1u;
+                if (idx < d.maxPtChunks) d.chunkQueue[idx] = d.tablePool[r.tableOff + j];
+            }
+            d.numPoints[node] = 0;
+            d.numPointChunks[node] = 0;
+            d.ptTableOff[node] = kNone;
+            d.ptTableCap[node] = 0;
+            uint32_t g = d.grid[node];
+            if (g == kNone) {
+                g = arenaAlloc(d, kGridUnits);
+                d.grid[node] = g;
+                atomicAdd(&c->numGrids, 1u);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
+                          (unsigned long long)refAllocSize(kGridBytes));
+            }
+            r.grid = g;
+            d.splitRecs[k] = r;
+            if (d.dirtyStamp[node] != c->buildStamp) {
+                d.dirtyStamp[node] = c->buildStamp;
+                const uint32_t di = atomicAdd(&c->numDirty, 1u);
+                if (di < d.maxNodes) d.dirtyList[di] = node;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_runPts += totPts;
+            s_runChunks += totCh;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        c->numNodes = nn + 8u * acc;
+        c->numSplit = acc;
+        c->spillChunkTotal = s_runChunks;
+        uint32_t total = spilledBefore + s_runPts;
+        if (total > d.spillCap) {
+            atomicOr(&c->overflowFlags, (uint32_t)kOvfSpilled);
+            total = d.spillCap;
+        }
+        c->numSpilled = total;
+        c->nodesSplit += acc;
+        c->numSpill = 0;
+        c->iter += 1;
+    }
+}
+
+// The split nodes' stored points move to the spill list (remolod_octree.cu:250-285)
+// and their grids are zeroed (:372-387). Work items: one per stored chunk, then
+// one per grid. Any grid size; items are strided over blocks.
+__global__ void __launch_bounds__(256) k_spill_copy(Dev d) {
+    const Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t nsplit = c->numSplit;
+    const uint32_t nchunk = c->spillChunkTotal;
+    const uint32_t items = nchunk + nsplit;
+    for (uint32_t w = blockIdx.x; w < items; w += gridDim.x) {
+        if (w < nchunk) {
+            // binary search for the record holding work item w
+            uint32_t lo = 0, hi = nsplit;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (d.splitRecs[mid].chunkBase <= w) lo = mid;
+                else hi = mid;
+            }
+            const SplitRec r = d.splitRecs[lo];
+            const uint32_t j = w - r.chunkBase;
+            const uint32_t phys = d.tablePool[r.tableOff + j];
+            if (phys == kNone) continue;
+            const uint32_t first = j * d.ppc;
+            uint32_t last = first + d.ppc;
+            if (last > r.numPoints) last = r.numPoints;
+            for (uint32_t s = first + threadIdx.x; s < last; s += blockDim.x) {
+                const uint32_t slot = r.spillBase + s;
+                if (slot >= d.spillCap) break;
+                d.spillPts[slot] = chunkPoints(d, phys)[s - first];
+                d.spillIdx[slot] = chunkIndices(d, phys)[s - first];
+                d.spillLeaf[slot] = r.node;
+            }
+        } else {
+            const SplitRec r = d.splitRecs[w - nchunk];
+            if (r.grid == kNone) continue;
+            uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, r.grid));
+            const uint4 z = make_uint4(0, 0, 0, 0);
+            for (uint32_t q = threadIdx.x; q < kGridWords / 4u; q += blockDim.x) g[q] = z;
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t hashSlot(unsigned long long key, uint32_t mask) {
+    unsigned long long h = key * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 32;
+    return (uint32_t)h & mask;
+}
+
+// Inserts (key -> min val) into the per-batch cell table.
+__device__ void hashInsert(const Dev& d, unsigned long long key, unsigned long long val) {
+    uint32_t slot = hashSlot(key, d.hashMask);
+    for (uint32_t probe = 0; probe < 256u; probe++) {
+        unsigned long long cur = d.hashKeys[slot];
+        if (cur == kHashEmpty) {
+            cur = atomicCAS(&d.hashKeys[slot], kHashEmpty, key);
+            if (cur == kHashEmpty) {
+                const uint32_t e = atomicAdd(&d.ctr->numNew, 1u);
+                if (e < d.newCap) d.hashNew[e] = slot;
+                else atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
+                cur = key;
+            }
+        }
+        if (cur == key) {
+            if (d.voxelMode == 0u) atomicMin(&d.hashVals[slot], val);
+            else atomicCAS(&d.hashVals[slot], kHashEmpty, val);
+            return;
+        }
+        slot = (slot + 1u) & d.hashMask;
+    }
+    atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
+}
+
+// voxelSampling (remolod_octree.cu:677-740) + sampleVoxel's test (:95-119):
+// every (point, level) pair whose cell bit was clear before this batch is a
+// candidate; the table keeps, per cell, the lowest global point index reaching
+// it (or the first to arrive). Bits are not written here, so every pair sees
+// the pre-batch grid, and the set of new cells is exactly the reference's.
+__global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    const Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
+    const uint32_t total = n + ns;
+    const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t lane = laneId();
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        bool active = i < total;
+        Point p = {0.f, 0.f, 0.f, 0u};
+        uint32_t gidx = 0;
+        if (i < n) {
+            p = loadPoint(pts + i);
+            gidx = firstIndex + i;
+        } else if (active) {
+            p = d.spillPts[i - n];
+            gidx = d.spillIdx[i - n];
+        }
+        uint32_t x20 = 0, y20 = 0, z20 = 0, x28 = 0, y28 = 0, z28 = 0;
+        if (active) {
+            x20 = quant20(p.x, d.boxMin[0], d.octreeSize);
+            y20 = quant20(p.y, d.boxMin[1], d.octreeSize);
+            z20 = quant20(p.z, d.boxMin[2], d.octreeSize);
+            x28 = quant28(p.x, d.boxMin[0], d.octreeSize);
+            y28 = quant28(p.y, d.boxMin[1], d.octreeSize);
+            z28 = quant28(p.z, d.boxMin[2], d.octreeSize);
+        }
+        uint32_t cur = 0;
+        for (uint32_t level = 0; level < (uint32_t)kMaxDepth; level++) {
+            if (!__any_sync(0xFFFFFFFFu, active)) break;
+            unsigned long long key = kHashEmpty;
+            if (active) {
+                const uint32_t g = __ldg(&d.grid[cur]);
+                if (g != kNone) {
+                    const uint32_t sh = (uint32_t)kMaxDepth + 1u - level;
+                    const uint32_t px = (x28 >> sh) & 127u, py = (y28 >> sh) & 127u,
+                                   pz = (z28 >> sh) & 127u;
+                    const uint32_t vi = px + py * 128u + pz * 16384u;
+                    const uint32_t word = __ldg(gridWordsAt(d, g) + (vi >> 5));
+                    if ((word & (1u << (vi & 31u))) == 0u)
+                        key = ((unsigned long long)cur << 21) | (unsigned long long)vi;
+                }
+                const int32_t nx = __ldg(&d.child[cur * 8u + childIndex(x20, y20, z20, level)]);
+                if (nx < 0) active = false;
+                else cur = (uint32_t)nx;
+            }
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+            if (key != kHashEmpty) {
+                int leader;
+                if (d.voxelMode == 0u) {
+                    const uint32_t mn = __reduce_min_sync(peers, gidx);
+                    leader = (gidx == mn) ? (int)lane : -1;
+                } else {
+                    leader = (lane == (uint32_t)(__ffs(peers) - 1)) ? (int)lane : -1;
+                }
+                if (leader == (int)lane)
+                    hashInsert(d, key, ((unsigned long long)gidx << 32) | p.color);
+            }
+        }
+    }
+}
+
+// Sets the new cells' bits and gives each new voxel its slot in its node
+// (sampleVoxel :119-138). Keys are unique, so every bit is set exactly once.
+__global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
+    const Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nnew; e += gridDim.x * blockDim.x) {
+        const uint32_t slot = d.hashNew[e];
+        const unsigned long long key = d.hashKeys[slot];
+        const uint32_t node = (uint32_t)(key >> 21);
+        const uint32_t vi = (uint32_t)(key & 0x1FFFFFull);
+        const uint32_t g = d.grid[node];
+        atomicOr(gridWordsAt(d, g) + (vi >> 5), 1u << (vi & 31u));
+        d.hashNewNode[e] = node;
+        d.hashNewSlot[e] = atomicAdd(&d.numVoxels[node], 1u);
+    }
+}
+
+// Grows a node's chunk table to hold `need` entries, keeping the first `keep`.
+__device__ bool ensureTable(const Dev& d, uint32_t* offArr, uint32_t* capArr, uint32_t node,
+                            uint32_t need, uint32_t keep) {
+    const uint32_t cap = capArr[node];
+    if (need <= cap) return true;
+    uint32_t ncap = 64u;
+    while (ncap < need) ncap <<= 1;
+    const uint32_t off = atomicAdd(&d.ctr->tableBump, ncap);
+    if ((uint64_t)off + ncap > d.tablePoolCap) {
+        atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfTables);
+        return false;
+    }
+    const uint32_t old = offArr[node];
+    for (uint32_t j = 0; j < keep && old != kNone; j++) d.tablePool[off + j] = d.tablePool[old + j];
+    offArr[node] = off;
+    capArr[node] = ncap;
+    return true;
+}
+
+__device__ __forceinline__ bool isLeaf(const Dev& d, uint32_t node) {
+    const int4* row = reinterpret_cast<const int4*>(d.child + node * 8u);
+    const int4 a = row[0], b = row[1];
+    return (a.x & a.y & a.z & a.w & b.x & b.y & b.z & b.w) == -1;
+}
+
+__device__ __forceinline__ void markDirty(const Dev& d, uint32_t node) {
+    Counters* c = d.ctr;
+    if (d.dirtyStamp[node] == c->buildStamp) return;
+    d.dirtyStamp[node] = c->buildStamp;
+    const uint32_t di = atomicAdd(&c->numDirty, 1u);
+    if (di < d.maxNodes) d.dirtyList[di] = node;
+    else atomicOr(&c->overflowFlags, (uint32_t)kOvfDirty);
+}
+
+// allocatePointChunks (remolod_octree.cu:742-792) and allocateVoxelChunks
+// (:885-916), one thread per node. Chunk ids come from the recycled queue
+// first, then from the pool; the reference store's offset advances by one
+// chunk for every pool chunk, so memCapacityReached falls where it would.
+__global__ void __launch_bounds__(256) k_alloc_chunks(Dev d) {
+    Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t nn = c->numNodes;
+    const uint32_t poolBefore = c->chunkPoolSize;
+    const uint32_t ppc = d.ppc;
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < nn;
+         node += gridDim.x * blockDim.x) {
+        const uint32_t npts = d.numPoints[node], cnt = d.counter[node];
+        if (npts < cnt && isLeaf(d, node)) {
+            const uint32_t req = (cnt + ppc - 1u) / ppc;
+            const uint32_t ex = (npts + ppc - 1u) / ppc;
+            if (req > ex && ensureTable(d, d.ptTableOff, d.ptTableCap, node, req, ex)) {
+                const uint32_t off = d.ptTableOff[node];
+                for (uint32_t e = ex; e < req; e++) {
+                    const uint32_t idx = atomicAdd(&c->numAllocatedChunks, 1u);
+                    uint32_t phys;
+                    if (idx < poolBefore && idx < d.maxPtChunks) {
+                        phys = d.chunkQueue[idx];
+                    } else {
+                        phys = arenaAlloc(d, d.ptChunkUnits);
+                        atomicAdd(&c->numPtChunks, 1u);
+                        atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
+                                  (unsigned long long)refAllocSize(kRefChunkBytes));
+                    }
+                    d.tablePool[off + e] = phys;
+                }
+                d.numPointChunks[node] = req;
+            }
+            markDirty(d, node);
+        }
+        const uint32_t nv = d.numVoxels[node];
+        const uint32_t reqv = (nv + ppc - 1u) / ppc;
+        const uint32_t havev = d.numVoxelChunks[node];
+        if (reqv > havev && ensureTable(d, d.vxTableOff, d.vxTableCap, node, reqv, havev)) {
+            const uint32_t off = d.vxTableOff[node];
+            for (uint32_t e = havev; e < reqv; e++) {
+                const uint32_t phys = arenaAlloc(d, d.vxChunkUnits);
+                atomicAdd(&c->numVxChunks, 1u);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
+                          (unsigned long long)refAllocSize(kRefChunkBytes));
+                d.tablePool[off + e] = phys;
+            }
+            d.numVoxelChunks[node] = reqv;
+        }
+    }
+}
+
+// insertPoints (remolod_octree.cu:794-883): batch points, then spilled points,
+// each into the leaf expand left it in. Slots are handed out per warp and leaf.
+__global__ void __launch_bounds__(256) k_insert(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
+    const uint32_t total = n + ns;
+    const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t lane = laneId();
+    const uint32_t ppc = d.ppc;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t leaf = kNone, gidx = 0;
+        Point p = {0.f, 0.f, 0.f, 0u};
+        if (i < n) {
+            leaf = d.leafOf[i];
+            p = loadPoint(pts + i);
+            gidx = firstIndex + i;
+        } else if (i < total) {
+            const uint32_t j = i - n;
+            leaf = d.spillLeaf[j];
+            p = d.spillPts[j];
+            gidx = d.spillIdx[j];
+        }
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, leaf);
+        if (leaf == kNone) continue;
+        const int leader = __ffs(peers) - 1;
+        uint32_t slotBase = 0;
+        if ((int)lane == leader) slotBase = atomicAdd(&d.numPoints[leaf], (uint32_t)__popc(peers));
+        slotBase = __shfl_sync(peers, slotBase, leader);
+        const uint32_t slot = slotBase + __popc(peers & ((1u << lane) - 1u));
+        const uint32_t cap = d.numPointChunks[leaf] * ppc;
+        uint32_t phys = kNone;
+        if (slot < cap) phys = d.tablePool[d.ptTableOff[leaf] + slot / ppc];
+        if (phys == kNone) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(&c->droppedPoints), 1ull);
+            continue;
+        }
+        chunkPoints(d, phys)[slot % ppc] = p;
+        chunkIndices(d, phys)[slot % ppc] = gidx;
+    }
+}
+
+// insertVoxels (remolod_octree.cu:918-938): every new cell's voxel at its cell
+// centre (:124-134) with its representative's colour; then the table entry is
+// cleared for the next batch.
+__global__ void __launch_bounds__(256) k_vox_store(Dev d) {
+    const Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
+    const uint32_t ppc = d.ppc;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nnew; e += gridDim.x * blockDim.x) {
+        const uint32_t hs = d.hashNew[e];
+        const unsigned long long key = d.hashKeys[hs];
+        const unsigned long long val = d.hashVals[hs];
+        d.hashKeys[hs] = kHashEmpty;
+        d.hashVals[hs] = kHashEmpty;
+        const uint32_t node = d.hashNewNode[e];
+        const uint32_t s = d.hashNewSlot[e];
+        const uint32_t vi = (uint32_t)(key & 0x1FFFFFull);
+        const uint32_t px = vi & 127u, py = (vi >> 7) & 127u, pz = vi >> 14;
+        const uint32_t lv = d.level[node];
+        const float nodeSize = __fdiv_rn(d.octreeSize, __int_as_float((int)((127u + lv) << 23)));
+        const float mnx = __fmaf_rn((float)d.nodeX[node], nodeSize, d.boxMin[0]);
+        const float mny = __fmaf_rn((float)d.nodeY[node], nodeSize, d.boxMin[1]);
+        const float mnz = __fmaf_rn((float)d.nodeZ[node], nodeSize, d.boxMin[2]);
+        Point v;
+        v.x = __fadd_rn(mnx, __fdiv_rn(__fmul_rn(nodeSize, __fadd_rn((float)px, 0.5f)), 128.0f));
+        v.y = __fadd_rn(mny, __fdiv_rn(__fmul_rn(nodeSize, __fadd_rn((float)py, 0.5f)), 128.0f));
+        v.z = __fadd_rn(mnz, __fdiv_rn(__fmul_rn(nodeSize, __fadd_rn((float)pz, 0.5f)), 128.0f));
+        v.color = (uint32_t)(val & 0xFFFFFFFFull);
+        atomicAdd(&d.numVoxelsStored[node], 1u);
+        if (s < d.numVoxelChunks[node] * ppc) {
+            const uint32_t phys = d.tablePool[d.vxTableOff[node] + s / ppc];
+            if (phys != kNone) chunkPoints(d, phys)[s % ppc] = v;
+        }
+    }
+}
+
+__global__ void k_batch_end(Dev d, uint32_t n) {
+    Counters* c = d.ctr;
+    if (c->batchStop) return;
+    if (c->numAllocatedChunks > c->chunkPoolSize) c->chunkPoolSize = c->numAllocatedChunks;
+    c->batchletIndex += 1;
+    c->numPointsProcessed += n;
+    c->spilledPointsTotal += c->numSpilled;
+    c->expandIters += c->iter < d.maxExpandIters ? c->iter : d.maxExpandIters;
+}
+
+// Stats sweep (remolod_octree.cu:1271-1310).
+__global__ void __launch_bounds__(256) k_sweep(Dev d) {
+    const uint32_t nn = d.ctr->numNodes;
+    const uint32_t ppc = d.ppc;
+    SweepStats* s = d.sweep;
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < nn;
+         node += gridDim.x * blockDim.x) {
+        const uint32_t np = d.numPoints[node];
+        const uint32_t lv = d.level[node];
+        atomicMax(&s->maxLevel, lv);
+        if (isLeaf(d, node)) {
+            atomicAdd(&s->numLeaves, 1u);
+            atomicAdd(&s->numPoints, (unsigned long long)np);
+            atomicAdd(&s->numChunksPoints, (np + ppc - 1u) / ppc);
+            atomicMax(&s->maxPointsPerNode, np);
+            if (d.counter[node] < np) atomicAdd(&s->counterUnderflows, 1u);
+            if (np > 0) atomicAdd(&s->numNonemptyLeaves, 1u);
+        } else {
+            const uint32_t nv = d.numVoxels[node];
+            atomicAdd(&s->numInner, 1u);
+            atomicAdd(&s->numVoxels, (unsigned long long)nv);
+            atomicAdd(&s->numChunksVoxels, (nv + ppc - 1u) / ppc);
+        }
+    }
+}
+
+// reset (remolod_reset.cu:41-85): the root, its grid, and the counters.
+__global__ void k_reset_root(Dev d) {
+    Counters* c = d.ctr;
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        Counters z = {};
+        z.buildStamp = c->buildStamp;
+        *c = z;
+        c->refOffset = 16;
+        c->numNodes = 1;
+        for (int q = 0; q < 8; q++) d.child[q] = -1;
+        d.counter[0] = 0;
+        d.numPoints[0] = 0;
+        d.level[0] = 0;
+        d.nodeX[0] = d.nodeY[0] = d.nodeZ[0] = 0;
+        d.grid[0] = 0;  // the root grid is the arena's first allocation
+        d.numVoxels[0] = 0;
+        d.numVoxelsStored[0] = 0;
+        d.numPointChunks[0] = 0;
+        d.numVoxelChunks[0] = 0;
+        d.ptTableOff[0] = kNone;
+        d.ptTableCap[0] = 0;
+        d.vxTableOff[0] = kNone;
+        d.vxTableCap[0] = 0;
+        d.splitIter[0] = 0;
+        d.dirtyStamp[0] = 0;
+        AccumI za = {};
+        d.accum[0] = za;
+        c->arenaBump = kGridUnits;
+        c->numGrids = 1;
+        c->refOffset += refAllocSize(kGridBytes);
+    }
+    uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, 0));
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < kGridWords / 4u;
+         q += gridDim.x * blockDim.x)
+        g[q] = z;
+}
+
+// ------------------------------------------------------------------ launches
+
+void launchBatchBegin(const Dev& d, cudaStream_t s) { k_batch_begin<<<1, 1, 0, s>>>(d); }
+void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
+    k_count_first<<<grid, 256, 0, s>>>(d, pts, n);
+}
+void launchRecount(const Dev& d, const Point* pts, uint32_t n, uint32_t prevStamp, int grid,
+                   cudaStream_t s) {
+    k_recount<<<grid, 256, 0, s>>>(d, pts, n, prevStamp);
+}
+void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s) { k_split<<<1, 1024, 0, s>>>(d, stamp); }
+void launchSpillCopy(const Dev& d, int grid, cudaStream_t s) { k_spill_copy<<<grid, 256, 0, s>>>(d); }
+void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
+    k_vox_sample<<<grid, 256, 0, s>>>(d, pts, n);
+}
+void launchVoxCommit(const Dev& d, int grid, cudaStream_t s) { k_vox_commit<<<grid, 256, 0, s>>>(d); }
+void launchAllocChunks(const Dev& d, int grid, cudaStream_t s) { k_alloc_chunks<<<grid, 256, 0, s>>>(d); }
+void launchInsert(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
+    k_insert<<<grid, 256, 0, s>>>(d, pts, n);
+}
+void launchVoxStore(const Dev& d, int grid, cudaStream_t s) { k_vox_store<<<grid, 256, 0, s>>>(d); }
+void launchBatchEnd(const Dev& d, uint32_t n, cudaStream_t s) { k_batch_end<<<1, 1, 0, s>>>(d, n); }
+void launchSweep(const Dev& d, int grid, cudaStream_t s) { k_sweep<<<grid, 256, 0, s>>>(d); }
+void launchResetRoot(const Dev& d, int grid, cudaStream_t s) { k_reset_root<<<grid, 256, 0, s>>>(d); }
+
+}  // namespace rb

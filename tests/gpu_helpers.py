@@ -1,0 +1,111 @@
+"""Shared helpers of the GPU parity tests: build the same cloud through the
+CUDA path (C ABI) and through the CPU oracle, and compare them."""
+import numpy as np
+
+from oracle import binding as ob
+
+
+def build_gpu(cloud, bmin, bmax, batch_size, budget=0, per_call=20, **cfg):
+    from remobench_b200.lod import Context, DeviceRing
+    slot_cap = cfg.pop("slot_capacity", batch_size)
+    ctx = Context(slot_capacity=slot_cap, time_budget_ms=0.0, max_batches_per_build=per_call, **cfg)
+    ctx.allocate(len(cloud), bmin, bmax, budget)
+    ring = DeviceRing(cloud, batch_size, slots=ctx.cfg.ring_slots, slot_capacity=slot_cap)
+    consumed, calls = 0, 0
+    while consumed < ring.num_batches:
+        ring.upload_window(consumed)
+        r = ctx.build(ring.ring, ring.sizes, ring.uploaded, ring.num_batches)
+        calls += 1
+        if r.batches_this_call == 0:
+            break
+        consumed = r.batches_consumed
+    return ctx, calls
+
+
+def build_oracle(cloud, bmin, bmax, batch_size, **cfg):
+    t = ob.Tree(**cfg)
+    t.reset(bmin, bmax)
+    for b in range((len(cloud) + batch_size - 1) // batch_size):
+        if t.add_batch(cloud[b * batch_size:(b + 1) * batch_size]) != 0:
+            break
+    t.sweep()
+    return t
+
+
+NODE_FIELDS = ["counter", "num_points", "level", "X", "Y", "Z", "num_voxels", "num_point_chunks",
+               "num_voxel_chunks", "is_leaf"]
+
+
+def compare_nodes(ctx, tree):
+    g = ctx.nodes()
+    o = tree.node_table()
+    assert len(g) == len(o), (len(g), len(o))
+    assert np.array_equal(g["child"], o["child"])
+    for f in NODE_FIELDS:
+        assert np.array_equal(g[f], o[f]), f
+    assert np.array_equal(g["has_grid"], (o["grid"] >= 0).astype(np.uint32))
+    return g
+
+
+def _rows(a):
+    return a.view(np.uint32).reshape(-1, 4)
+
+
+def compare_points(ctx, tree, nodes):
+    for i in np.nonzero(nodes["num_points"])[0]:
+        i = int(i)
+        gp, gi = ctx.node_points(i)
+        op, oi = tree.leaf_points(i)
+        assert len(gp) == len(op), i
+        a, b = np.argsort(gi, kind="stable"), np.argsort(oi, kind="stable")
+        assert np.array_equal(gi[a], oi[b]), i
+        assert np.array_equal(_rows(gp)[a], _rows(op)[b]), i
+
+
+def compare_voxels(ctx, tree, nodes, colours=True):
+    for i in np.nonzero(nodes["num_voxels"])[0]:
+        i = int(i)
+        gv = _rows(ctx.node_voxels(i))
+        ov = _rows(tree.node_voxels(i))
+        assert len(gv) == len(ov), i
+        if not colours:
+            gv, ov = gv[:, :3], ov[:, :3]
+        ga = gv[np.lexsort(gv.T[::-1])]
+        oa = ov[np.lexsort(ov.T[::-1])]
+        assert np.array_equal(ga, oa), i
+
+
+def compare_grids(ctx, tree, nodes):
+    for i in np.nonzero(nodes["has_grid"])[0]:
+        i = int(i)
+        assert np.array_equal(ctx.node_grid(i), tree.node_grid(i)), i
+
+
+STAT_FIELDS = ["num_points", "num_voxels", "num_inner", "num_leaves", "num_nonempty_leaves",
+               "num_chunks_points", "num_chunks_voxels", "batchlet_index", "num_allocated_chunks",
+               "chunk_pool_size", "mem_capacity_reached", "counter_underflows", "dropped_points",
+               "nodes_split", "spilled_points", "num_grids", "overflow_flags", "max_points_per_node"]
+
+
+def compare_stats(ctx, tree):
+    g = ctx.stats()
+    o = tree.stats()
+    for f in STAT_FIELDS:
+        assert getattr(g, f) == getattr(o, f), (f, getattr(g, f), getattr(o, f))
+    assert g.num_nodes == o.num_nodes
+    assert g.persistent_offset == o.persistent_offset
+    assert g.num_points_ingested == o.num_points_processed
+    return g
+
+
+def compare_accums(ctx, tree):
+    ga = ctx.accums()
+    for i in range(tree.num_nodes()):
+        a = tree.accum_i(i)
+        g = ga[i]
+        assert list(g["s1"]) == list(a.s1), i
+        assert list(g["s2_lo"]) == list(a.s2_lo), i
+        assert list(g["s2_hi"]) == list(a.s2_hi), i
+        assert list(g["c1"]) == list(a.c1), i
+        assert list(g["c2"]) == list(a.c2), i
+        assert g["count"] == a.count, i

@@ -1,0 +1,84 @@
+"""Update + Accumulate on the B200 against the CPU oracle: bit-exact node
+set, per-node point multisets, occupancy bits, voxels (lowest-index rule),
+statistics, and exact integer accumulators."""
+import numpy as np
+import pytest
+
+from gpu_helpers import (build_gpu, build_oracle, compare_accums, compare_grids, compare_nodes,
+                         compare_points, compare_stats, compare_voxels)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c1_pair(c1_cloud):
+    cfg, cloud, bmin, bmax = c1_cloud
+    ctx, _ = build_gpu(cloud, bmin, bmax, cfg.batch_size)
+    tree = build_oracle(cloud, bmin, bmax, cfg.batch_size)
+    tree.accumulate(8)
+    return ctx, tree
+
+
+def test_tree_bit_exact(c1_pair):
+    ctx, tree = c1_pair
+    nodes = compare_nodes(ctx, tree)
+    assert len(nodes) > 100
+
+
+def test_stats_and_store_offsets(c1_pair):
+    ctx, tree = c1_pair
+    s = compare_stats(ctx, tree)
+    assert s.num_points == 8 * 262144
+
+
+def test_point_multisets(c1_pair):
+    ctx, tree = c1_pair
+    compare_points(ctx, tree, ctx.nodes())
+
+
+def test_voxels_lowest_index(c1_pair):
+    ctx, tree = c1_pair
+    compare_voxels(ctx, tree, ctx.nodes())
+
+
+def test_occupancy_grids(c1_pair):
+    ctx, tree = c1_pair
+    compare_grids(ctx, tree, ctx.nodes())
+
+
+def test_accumulators_exact(c1_pair):
+    ctx, tree = c1_pair
+    compare_accums(ctx, tree)
+
+
+def test_batch_grouping_and_host_ingest_give_same_tree(c1_cloud, c1_pair):
+    cfg, cloud, bmin, bmax = c1_cloud
+    ctx, tree = c1_pair
+    ref = ctx.nodes()
+    # three batches per build call instead of all eight
+    ctx3, calls = build_gpu(cloud, bmin, bmax, cfg.batch_size, per_call=3)
+    assert calls >= 3
+    assert np.array_equal(ctx3.nodes(), ref)
+    compare_accums(ctx3, tree)
+    # end-to-end path from host memory through the copy stream
+    from remobench_b200.lod import Context
+    ch = Context(slot_capacity=cfg.batch_size, time_budget_ms=0.0)
+    ch.allocate(len(cloud), bmin, bmax)
+    r = ch.ingest_host(cloud, cfg.batch_size)
+    assert r.batches_consumed == 8
+    assert np.array_equal(ch.nodes(), ref)
+    compare_accums(ch, tree)
+
+
+def test_first_come_voxels_are_members_of_their_cell(c1_cloud, c1_pair):
+    cfg, cloud, bmin, bmax = c1_cloud
+    _, tree = c1_pair
+    sub = cloud[: 2 * cfg.batch_size]
+    ctx, _ = build_gpu(sub, bmin, bmax, cfg.batch_size, voxel_mode=1)
+    t2 = build_oracle(sub, bmin, bmax, cfg.batch_size)
+    nodes = compare_nodes(ctx, t2)
+    compare_voxels(ctx, t2, nodes, colours=False)
+    colours = set(np.unique(sub["color"]).tolist())
+    for i in np.nonzero(nodes["num_voxels"])[0][:50]:
+        for v in ctx.node_voxels(int(i)):
+            assert int(v["color"]) in colours

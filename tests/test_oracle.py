@@ -1,0 +1,208 @@
+"""The CPU oracle against hand-derived known answers and the reference's own
+invariants (the reference ships no tests or fixtures for this path; its
+structural pins are on lidar files that are not distributed)."""
+import numpy as np
+import pytest
+
+from oracle import binding as ob
+
+PT = ob.POINT_DTYPE
+
+
+def pts(rows):
+    a = np.zeros(len(rows), dtype=PT)
+    for i, (x, y, z, c) in enumerate(rows):
+        a[i] = (x, y, z, c)
+    return a
+
+
+def unit_tree(**cfg):
+    t = ob.Tree(**cfg)
+    t.reset((0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
+    return t
+
+
+def test_child_index_bit_order():
+    # remolod_octree.cu:184-192: child = (x << 2) | (y << 1) | z of bit (19 - level).
+    # (0.75, 0.25, 0.5) in a unit cube: X20 = 786432 (bit19=1), Y20 = 262144 (0), Z20 = 524288 (1) -> child 5.
+    t = unit_tree(max_points_per_node=4)
+    cloud = pts([(0.75, 0.25, 0.5, 1), (0.25, 0.25, 0.25, 2), (0.25, 0.75, 0.25, 3),
+                 (0.75, 0.75, 0.75, 4), (0.25, 0.25, 0.75, 5)])
+    assert t.add_batch(cloud) == 0
+    t.sweep()
+    root = t.node(0)
+    assert not root.is_leaf
+    kids = list(root.child)
+    assert kids == list(range(1, 9))  # the first split takes ids 1..8
+    c5 = t.node(kids[5])
+    assert (c5.level, c5.X, c5.Y, c5.Z) == (1, 1, 0, 1)
+    assert c5.num_points == 1 and c5.counter == 1
+    p, idx = t.leaf_points(kids[5])
+    assert list(idx) == [0]
+    assert [t.node(k).num_points for k in kids] == [1, 1, 1, 0, 0, 1, 0, 1]
+
+
+def test_root_voxel_cell_and_centre():
+    # sampleVoxel (remolod_octree.cu:103-133) at the root, level 0: cell = pFull >> 21.
+    # pFull = u32(2^28 * 0.75) = 201326592 -> 96; 0.25 -> 32; 0.5 -> 64.
+    # centre x = 0 + 1 * (96 + 0.5) / 128 = 0.75390625.
+    t = unit_tree(max_points_per_node=4)
+    cloud = pts([(0.75, 0.25, 0.5, 0xAABBCCDD)] * 5)
+    t.add_batch(cloud)
+    g = t.node_grid(0)
+    vi = 96 + 32 * 128 + 64 * 16384
+    assert g[vi // 32] == (1 << (vi % 32))
+    assert int(np.count_nonzero(g)) == 1
+    v = t.node_voxels(0)
+    assert len(v) == 1
+    assert v[0]["x"] == np.float32(0.75390625)
+    assert v[0]["y"] == np.float32((32 + 0.5) / 128)
+    assert v[0]["z"] == np.float32((64 + 0.5) / 128)
+    assert v[0]["color"] == 0xAABBCCDD
+
+
+def test_box_max_wraps_to_cell_zero():
+    # A point exactly on boxMax quantises to 2^20: the descent's per-level & 1
+    # wraps it to the low child (wiki/04_FixedDepthFindings.md:291-296), and
+    # its 2^28 cell index wraps to 0 at the root (% 128).
+    t = unit_tree(max_points_per_node=2)
+    cloud = pts([(1.0, 1.0, 1.0, 7), (1.0, 1.0, 1.0, 8), (1.0, 1.0, 1.0, 9)])
+    t.add_batch(cloud)
+    root = t.node(0)
+    assert not root.is_leaf
+    # child 0 (x=y=z=0) holds them, and so on down to MAX_DEPTH: every level wraps
+    c0 = t.node(root.child[0])
+    assert c0.counter == 3
+    g = t.node_grid(0)
+    assert g[0] & 1
+
+
+def test_lowest_index_representative():
+    t = unit_tree(max_points_per_node=8)
+    # 9 points in one root cell, different colours; the first (lowest index) wins
+    cloud = pts([(0.1, 0.1, 0.1 + 1e-6 * i, 100 + i) for i in range(9)])
+    t.add_batch(cloud)
+    v = t.node_voxels(0)
+    assert len(v) == 1 and v[0]["color"] == 100
+
+
+def test_spilled_points_keep_index_and_win_later_cells():
+    # batch 0 fills a leaf to the limit; batch 1 pushes it over: the stored points
+    # spill and re-insert into children with their original indices.
+    t = unit_tree(max_points_per_node=4)
+    b0 = pts([(0.6 + 0.01 * i, 0.6, 0.6, 10 + i) for i in range(4)])
+    b1 = pts([(0.6 + 0.01 * i, 0.6, 0.6, 20 + i) for i in range(2)])
+    t.add_batch(b0)
+    assert t.node(0).is_leaf
+    t.add_batch(b1)
+    t.sweep()
+    s = t.stats()
+    assert s.num_points == 6 and s.spilled_points == 4
+    seen = {}
+    for i in range(t.num_nodes()):
+        p, idx = t.leaf_points(i)
+        for q, k in zip(p, idx):
+            seen[int(k)] = int(q["color"])
+    assert seen == {0: 10, 1: 11, 2: 12, 3: 13, 4: 20, 5: 21}
+
+
+def test_node_pool_refusal_keeps_points():
+    t = unit_tree(max_points_per_node=2, max_nodes=9)
+    cloud = pts([(0.1 * (i % 9) + 0.05, 0.3, 0.3, i) for i in range(30)])
+    t.add_batch(cloud)
+    t.sweep()
+    s = t.stats()
+    assert s.node_pool_overflow == 1
+    assert s.num_nodes == 9
+    assert s.num_points == 30  # nothing dropped, nothing duplicated
+    assert s.dropped_points == 0
+
+
+def test_memory_check_truncates_between_batches():
+    # AllocatorGlobal offsets (utils.h.cu:195): root grid 262160 B after the 16-byte header;
+    # a capacity below offset + margin refuses the batch (remolod_octree.cu:1197-1210).
+    t = ob.Tree(persistent_capacity=16 + 262160 + 1000, safety_margin=1000)
+    t.reset((0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
+    assert t.stats().persistent_offset == 16 + 262160
+    cloud = pts([(0.5, 0.5, 0.5, 1)])
+    assert t.add_batch(cloud) == 1
+    assert t.stats().mem_capacity_reached == 1
+    assert t.stats().batchlet_index == 0
+
+
+def test_config1_invariants(c1_cloud):
+    cfg, cloud, bmin, bmax = c1_cloud
+    t = ob.Tree()
+    t.reset(bmin, bmax)
+    bs = cfg.batch_size
+    for b in range(8):
+        assert t.add_batch(cloud[b * bs:(b + 1) * bs]) == 0
+    t.sweep()
+    s = t.stats()
+    n = len(cloud)
+    # diagnostics() invariants (src/pipelines/RemolodPipeline.cpp:603-726)
+    assert s.num_points == n
+    assert s.counter_underflows == 0
+    assert s.dropped_points == 0 and s.overflow_flags == 0
+    assert s.num_inner + s.num_leaves == s.num_nodes
+    g = t.accumulate(8)
+    assert g.sum_leaf_counts == n
+    assert g.inner_with_sums == 0
+    # every input point is stored exactly once, with its global index
+    seen = np.zeros(n, dtype=np.int32)
+    nodes = t.node_table()
+    for i in np.nonzero(nodes["is_leaf"])[0]:
+        p, idx = t.leaf_points(int(i))
+        seen[idx] += 1
+        assert np.array_equal(p.view(np.uint32).reshape(-1, 4), cloud[idx].view(np.uint32).reshape(-1, 4))
+    assert np.all(seen == 1)
+    # leaves stay within the split limit unless they sit at MAX_DEPTH
+    assert np.all(nodes["num_points"][nodes["is_leaf"] == 1] <= 50000)
+
+
+def test_build_ring_equals_add_batch(c1_cloud):
+    cfg, cloud, bmin, bmax = c1_cloud
+    sub = cloud[: 4 * cfg.batch_size]
+    bs = cfg.batch_size
+    a = ob.Tree()
+    a.reset(bmin, bmax)
+    for b in range(4):
+        a.add_batch(sub[b * bs:(b + 1) * bs])
+    a.sweep()
+    # the same batches through kernel_construct's ring loop, two at a time
+    ring = np.zeros(50 * bs, dtype=ob.POINT_DTYPE)
+    sizes = np.zeros(50, dtype=np.uint32)
+    for b in range(4):
+        ring[b * bs:(b + 1) * bs] = sub[b * bs:(b + 1) * bs]
+        sizes[b] = bs
+    t = ob.Tree(slot_capacity=bs, max_batches_per_build=2)
+    t.reset(bmin, bmax)
+    assert t.build(ring, sizes, 4) == 2
+    assert t.build(ring, sizes, 4) == 2
+    assert np.array_equal(a.node_table(), t.node_table())
+
+
+def test_accumulate_watermark_is_incremental(c1_cloud):
+    cfg, cloud, bmin, bmax = c1_cloud
+    bs = cfg.batch_size
+    once = ob.Tree()
+    once.reset(bmin, bmax)
+    twice = ob.Tree()
+    twice.reset(bmin, bmax)
+    for b in range(3):
+        once.add_batch(cloud[b * bs:(b + 1) * bs])
+        twice.add_batch(cloud[b * bs:(b + 1) * bs])
+        twice.accumulate(b)
+    once.accumulate(2)
+    for i in range(once.num_nodes()):
+        a, b = once.accum_i(i), twice.accum_i(i)
+        assert bytes(a)[:-12] == bytes(b)[:-12]  # all sums and the count; not last_touched_batch
+
+
+def test_jacobi_known_eigenvalues():
+    e, v = ob.sym3_eig([2.0, 0.0, 0.0, 3.0, 0.0, 1.0])
+    assert np.allclose(e, [3.0, 2.0, 1.0])
+    assert np.allclose(np.abs(v), [0.0, 0.0, 1.0])
+    a = np.array([[4.0, 1.0, 0.5], [1.0, 3.0, 0.2], [0.5, 0.2, 1.0]])
+    e, _ = ob.sym3_eig([a[0, 0], a[0, 1], a[0, 2], a[1, 1], a[1, 2], a[2, 2]])
+    assert np.allclose(e, np.sort(np.linalg.eigvalsh(a))[::-1], rtol=1e-12)

@@ -213,6 +213,19 @@ typedef struct rb_node_info {
     uint32_t is_leaf;
 } rb_node_info;
 
+/* Per-kernel launch counts (always kept) and CUDA-event durations (kept
+ * while profiling is on; each launch is bracketed by events on the context's
+ * stream, so leave it off for timing whole calls). No reference counterpart:
+ * the reference times phases with %globaltimer marks inside its cooperative
+ * kernel (kernels/shared/remo_prelude.cuh:58-85). */
+typedef struct rb_kernel_profile {
+    char name[32];
+    uint64_t launches;
+    uint64_t timed_launches;
+    double total_ms;
+    uint64_t units;                  /* points (or pixels) handed to the kernel */
+} rb_kernel_profile;
+
 uint32_t rb_abi_version(void);
 const char* rb_status_string(rb_status s);
 void rb_config_defaults(rb_config* cfg);
@@ -269,6 +282,11 @@ rb_status rb_read_node_voxels(struct rb_ctx* ctx, uint32_t node, rb_point* vox, 
                               uint32_t* count);
 rb_status rb_read_node_grid(struct rb_ctx* ctx, uint32_t node, uint32_t* words65536);
 rb_status rb_read_accums(struct rb_ctx* ctx, rb_accum* out, uint32_t capacity, uint32_t* count);
+
+/* Kernel timing (see rb_kernel_profile). */
+rb_status rb_set_profiling(struct rb_ctx* ctx, int on);
+rb_status rb_read_profile(struct rb_ctx* ctx, rb_kernel_profile* out, uint32_t capacity, uint32_t* count);
+rb_status rb_reset_profile(struct rb_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -83,6 +83,11 @@ class NodeInfo(ctypes.Structure):
                 ("num_voxel_chunks", u32), ("is_leaf", u32)]
 
 
+class KernelProfile(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", u64), ("timed_launches", u64),
+                ("total_ms", ctypes.c_double), ("units", u64)]
+
+
 # name -> (restype, argtypes); the declarations of include/rb_capi.h
 _vp = ctypes.c_void_p
 SIGNATURES = {
@@ -107,6 +112,9 @@ SIGNATURES = {
     "rb_read_node_voxels": (i32, [_vp, u32, _vp, u32, ctypes.POINTER(u32)]),
     "rb_read_node_grid": (i32, [_vp, u32, _vp]),
     "rb_read_accums": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
+    "rb_set_profiling": (i32, [_vp, ctypes.c_int]),
+    "rb_read_profile": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
+    "rb_reset_profile": (i32, [_vp]),
 }
 
 _lib = None

@@ -18,7 +18,64 @@ using rb::Counters;
 using rb::Dev;
 using rb::kNone;
 
+// Per-kernel launch counts (always) and CUDA-event durations (when profiling).
+enum KernelId : int {
+    K_BUILD_BEGIN, K_BATCH_BEGIN, K_COUNT_FIRST, K_SPLIT, K_SPILL_COPY, K_RECOUNT, K_VOX_SAMPLE,
+    K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END, K_ACCUMULATE, K_ACCUM_VERIFY,
+    K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
+    K_RESOLVE, K_NUM
+};
+static const char* const kKernelNames[K_NUM] = {
+    "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
+    "k_vox_sample", "k_vox_commit", "k_alloc_chunks", "k_insert", "k_vox_store", "k_batch_end",
+    "k_accumulate", "k_accum_verify", "k_sweep", "k_reset_root", "k_fb_clear", "k_node_flags",
+    "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve"};
+
+struct Profiler {
+    bool on = false;
+    uint64_t launches[K_NUM] = {};
+    double ms[K_NUM] = {};
+    uint64_t timed[K_NUM] = {};
+    uint64_t units[K_NUM] = {};  // points (or pixels, nodes) handed to the kernel
+    std::vector<cudaEvent_t> pool;
+    struct Pending {
+        int id;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    cudaEvent_t take() {
+        if (pool.empty()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    void resolve() {
+        for (auto& p : pending) {
+            float t = 0.0f;
+            if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&t, p.a, p.b) == cudaSuccess) {
+                ms[p.id] += t;
+                timed[p.id] += 1;
+            }
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    ~Profiler() {
+        for (auto& p : pending) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
 struct rb_ctx {
+    Profiler prof;
     rb_config cfg{};
     std::string err;
     int device = 0;
@@ -96,10 +153,31 @@ int pointGrid(const rb_ctx* c, uint64_t n) {
     return (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (uint64_t)c->numSMs * 8));
 }
 
+// Launches `stmt` as kernel `id`, bracketed by events when profiling.
+#define LAUNCH(c, id, nunits, stmt)                                       \
+    do {                                                                  \
+        (c)->prof.launches[id] += 1;                                      \
+        (c)->prof.units[id] += (uint64_t)(nunits);                        \
+        if ((c)->prof.on) {                                               \
+            cudaEvent_t a_ = (c)->prof.take(), b_ = (c)->prof.take();     \
+            cudaEventRecord(a_, (c)->stream);                             \
+            stmt;                                                         \
+            cudaEventRecord(b_, (c)->stream);                             \
+            (c)->prof.pending.push_back({(id), a_, b_});                  \
+        } else {                                                          \
+            stmt;                                                         \
+        }                                                                 \
+    } while (0)
+
 rb_status readCounters(rb_ctx* c) {
     RB_CUDA(c, cudaMemcpyAsync(c->hostCtr, c->d.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, c->stream));
     RB_CUDA(c, cudaStreamSynchronize(c->stream));
     return RB_OK;
+}
+
+__global__ void k_build_begin(Counters* c) {
+    c->buildStamp += 1;
+    c->numDirty = 0;
 }
 
 // One batch through addBatch's phases (remolod_octree.cu:940-1060). Returns
@@ -113,8 +191,8 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
         RB_CUDA(c, cudaMemsetAsync(d.hashKeys, 0xFF, ((size_t)d.hashMask + 1) * 8, s));
         RB_CUDA(c, cudaMemsetAsync(d.hashVals, 0xFF, ((size_t)d.hashMask + 1) * 8, s));
     }
-    rb::launchBatchBegin(d, s);
-    rb::launchCountFirst(d, pts, n, pointGrid(c, n), s);
+    LAUNCH(c, K_BATCH_BEGIN, 1, rb::launchBatchBegin(d, s));
+    LAUNCH(c, K_COUNT_FIRST, n, rb::launchCountFirst(d, pts, n, pointGrid(c, n), s));
     const int fixedGrid = c->numSMs * 4;
     for (uint32_t iter = 1;; iter++) {
         rb_status st = readCounters(c);
@@ -125,33 +203,30 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
         }
         if (c->hostCtr->numSpill == 0) break;
         const uint32_t stamp = (batchIndex << 5) | iter;
-        rb::launchSplit(d, stamp, s);
-        rb::launchSpillCopy(d, fixedGrid, s);
+        LAUNCH(c, K_SPLIT, c->hostCtr->numSpill, rb::launchSplit(d, stamp, s));
+        LAUNCH(c, K_SPILL_COPY, 0, rb::launchSpillCopy(d, fixedGrid, s));
         if (iter >= c->cfg.max_expand_iters) break;
-        rb::launchRecount(d, pts, n, stamp, pointGrid(c, n), s);
+        LAUNCH(c, K_RECOUNT, n, rb::launchRecount(d, pts, n, stamp, pointGrid(c, n), s));
     }
     const uint64_t work = n;
-    rb::launchVoxSample(d, pts, n, pointGrid(c, work), s);
-    rb::launchVoxCommit(d, fixedGrid, s);
-    rb::launchAllocChunks(d, fixedGrid, s);
-    rb::launchInsert(d, pts, n, pointGrid(c, work), s);
-    rb::launchVoxStore(d, fixedGrid, s);
-    rb::launchBatchEnd(d, n, s);
+    LAUNCH(c, K_VOX_SAMPLE, n, rb::launchVoxSample(d, pts, n, pointGrid(c, work), s));
+    LAUNCH(c, K_VOX_COMMIT, 0, rb::launchVoxCommit(d, fixedGrid, s));
+    LAUNCH(c, K_ALLOC_CHUNKS, 0, rb::launchAllocChunks(d, fixedGrid, s));
+    LAUNCH(c, K_INSERT, n, rb::launchInsert(d, pts, n, pointGrid(c, work), s));
+    LAUNCH(c, K_VOX_STORE, 0, rb::launchVoxStore(d, fixedGrid, s));
+    LAUNCH(c, K_BATCH_END, 1, rb::launchBatchEnd(d, n, s));
     RB_CUDA(c, cudaGetLastError());
     return RB_OK;
-}
-
-__global__ void k_build_begin(Counters* c) {
-    c->buildStamp += 1;
-    c->numDirty = 0;
 }
 
 rb_status accumulate(rb_ctx* c, uint32_t batchIndex) {
     const Dev& d = c->d;
     // sumLeafCounts .. innerWithSums restart per launch (RemolodPipeline.cpp:251-256)
     RB_CUDA(c, cudaMemsetAsync(reinterpret_cast<uint8_t*>(d.accumGlobals) + 16, 0, 20, c->stream));
-    rb::launchAccumulate(d, batchIndex, c->accumAll ? 0 : 1, c->numSMs * 8, c->stream);
-    rb::launchAccumVerify(d, c->numSMs * 2, c->stream);
+    LAUNCH(c, K_ACCUMULATE, 0, rb::launchAccumulate(d, batchIndex, c->accumAll ? 0 : 1, c->numSMs * 8, c->stream));
+    LAUNCH(c, K_ACCUM_VERIFY, 0, rb::launchAccumVerify(d, c->numSMs * 2, c->stream));
+    // the dirty list restarts: it names the nodes touched since this fold
+    LAUNCH(c, K_BUILD_BEGIN, 1, (k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr)));
     RB_CUDA(c, cudaGetLastError());
     c->accumAll = false;
     return RB_OK;
@@ -419,7 +494,7 @@ rb_status rb_reset(rb_ctx* c) {
     if (!c->allocated) return fail(c, RB_ERR_STATE, "reset before allocate");
     if (c->cfg.pipeline == RB_PIPELINE_FLAT) return RB_OK;
     RB_CUDA(c, cudaSetDevice(c->device));
-    rb::launchResetRoot(c->d, c->numSMs * 2, c->stream);
+    LAUNCH(c, K_RESET_ROOT, 1, rb::launchResetRoot(c->d, c->numSMs * 2, c->stream));
     RB_CUDA(c, cudaMemsetAsync(c->d.accumGlobals, 0, sizeof(rb::AccumGlobals), c->stream));
     RB_CUDA(c, cudaGetLastError());
     RB_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -435,7 +510,7 @@ static rb_status buildFrom(rb_ctx* c, const rb::Point* ring, const uint32_t* siz
     const uint32_t avail = numUploaded > first ? numUploaded - first : 0u;
     const uint32_t nb = std::min(avail, maxBatches);
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
-    k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr);
+    LAUNCH(c, K_BUILD_BEGIN, 1, (k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr)));
     uint32_t done = 0;
     bool stopped = false;
     for (uint32_t b = first; b < first + nb; b++) {
@@ -506,7 +581,7 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
     const uint64_t nb = (n + batchSize - 1) / batchSize;
     const uint32_t S = c->ingestSlots;
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
-    k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr);
+    LAUNCH(c, K_BUILD_BEGIN, 1, (k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr)));
     // the copy stream fills slot (b % S) once the compute stream released it
     auto issueCopy = [&](uint64_t b) -> rb_status {
         const uint32_t slot = (uint32_t)(b % S);
@@ -524,6 +599,8 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
     }
     uint32_t done = 0;
     bool stopped = false;
+    const bool accumOn = c->cfg.accumulate && c->cfg.pipeline == RB_PIPELINE_REMOLOD;
+    bool pendingFold = false;
     for (uint64_t b = 0; b < nb; b++) {
         const uint32_t slot = (uint32_t)(b % S);
         const uint64_t first = b * batchSize;
@@ -540,11 +617,19 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
             st = issueCopy(b + S);
             if (st != RB_OK) return st;
         }
+        // Accumulate at the frame cadence: after every max_batches_per_build batches
+        if (accumOn && (done % std::max<uint32_t>(c->cfg.max_batches_per_build, 1)) == 0) {
+            st = accumulate(c, c->batchesConsumed);
+            if (st != RB_OK) return st;
+            pendingFold = false;
+        } else {
+            pendingFold = true;
+        }
     }
-    if (c->cfg.accumulate && c->cfg.pipeline == RB_PIPELINE_REMOLOD) {
+    if (accumOn && pendingFold) {
         rb_status st = accumulate(c, c->batchesConsumed);
         if (st != RB_OK) return st;
-    } else if (done > 0) {
+    } else if (!accumOn && done > 0) {
         c->accumAll = true;
     }
     RB_CUDA(c, cudaEventRecord(c->evStop, c->stream));
@@ -603,10 +688,10 @@ static rb_status finishFrame(rb_ctx* c, const rb_frame* f, unsigned long long* f
             c->fbTmpPixels = npx;
         }
         RB_CUDA(c, cudaMemcpyAsync(c->fbTmp, fb, npx * 8, cudaMemcpyDeviceToDevice, c->stream));
-        rb::launchEdl(c->fbTmp, fb, (uint32_t)f->width, (uint32_t)f->height, f->edl_strength,
-                      c->numSMs * 8, c->stream);
+        LAUNCH(c, K_EDL, npx, rb::launchEdl(c->fbTmp, fb, (uint32_t)f->width, (uint32_t)f->height,
+                                            f->edl_strength, c->numSMs * 8, c->stream));
     }
-    if (rgba) rb::launchResolve(fb, rgba, npx, c->numSMs * 8, c->stream);
+    if (rgba) LAUNCH(c, K_RESOLVE, npx, rb::launchResolve(fb, rgba, npx, c->numSMs * 8, c->stream));
     return RB_OK;
 }
 
@@ -621,11 +706,13 @@ rb_status rb_render(rb_ctx* c, const rb_frame* f, uint64_t fbDev, uint64_t rgbaD
     const rb::Frame fr = toFrame(f);
     const uint32_t cap = std::max<uint32_t>(c->cfg.drawlist_capacity, 1);
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
-    rb::launchFbClear(fb, npx, c->numSMs * 8, c->stream);
-    rb::launchNodeFlags(c->d, fr, c->vis, c->large, reinterpret_cast<const uint8_t*>(forceDev), c->rs,
-                        c->numSMs * 4, c->stream);
-    rb::launchFrontier(c->d, c->vis, c->large, c->rs, c->items, cap, c->numSMs * 4, c->stream);
-    rb::launchRaster(c->d, fr, fb, c->rs, c->items, cap, c->numSMs * 8, c->stream);
+    LAUNCH(c, K_FB_CLEAR, npx, rb::launchFbClear(fb, npx, c->numSMs * 8, c->stream));
+    LAUNCH(c, K_NODE_FLAGS, 0, rb::launchNodeFlags(c->d, fr, c->vis, c->large,
+                                                   reinterpret_cast<const uint8_t*>(forceDev), c->rs,
+                                                   c->numSMs * 4, c->stream));
+    LAUNCH(c, K_FRONTIER, 0, rb::launchFrontier(c->d, c->vis, c->large, c->rs, c->items, cap, c->numSMs * 4,
+                                                c->stream));
+    LAUNCH(c, K_RASTER, 0, rb::launchRaster(c->d, fr, fb, c->rs, c->items, cap, c->numSMs * 8, c->stream));
     rb_status st = finishFrame(c, f, fb, reinterpret_cast<uint32_t*>(rgbaDev), npx);
     if (st != RB_OK) return st;
     RB_CUDA(c, cudaGetLastError());
@@ -655,8 +742,11 @@ rb_status rb_render_flat(rb_ctx* c, const rb_frame* f, uint64_t pointsDev, uint6
     auto* fb = reinterpret_cast<unsigned long long*>(fbDev);
     const rb::Frame fr = toFrame(f);
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
-    rb::launchFbClear(fb, npx, c->numSMs * 8, c->stream);
-    if (n) rb::launchRasterFlat(fr, fb, reinterpret_cast<const rb::Point*>(pointsDev), n, c->numSMs * 16, c->stream);
+    LAUNCH(c, K_FB_CLEAR, npx, rb::launchFbClear(fb, npx, c->numSMs * 8, c->stream));
+    if (n)
+        LAUNCH(c, K_RASTER_FLAT, n,
+               rb::launchRasterFlat(fr, fb, reinterpret_cast<const rb::Point*>(pointsDev), n, c->numSMs * 16,
+                                    c->stream));
     rb_status st = finishFrame(c, f, fb, reinterpret_cast<uint32_t*>(rgbaDev), npx);
     if (st != RB_OK) return st;
     RB_CUDA(c, cudaGetLastError());
@@ -681,7 +771,7 @@ rb_status rb_read_stats(rb_ctx* c, rb_stats* o) {
     if (c->cfg.pipeline == RB_PIPELINE_FLAT) return RB_OK;
     RB_CUDA(c, cudaSetDevice(c->device));
     RB_CUDA(c, cudaMemsetAsync(c->d.sweep, 0, sizeof(rb::SweepStats), c->stream));
-    rb::launchSweep(c->d, c->numSMs * 4, c->stream);
+    LAUNCH(c, K_SWEEP, 0, rb::launchSweep(c->d, c->numSMs * 4, c->stream));
     RB_CUDA(c, cudaGetLastError());
     RB_CUDA(c, cudaMemcpyAsync(c->hostSweep, c->d.sweep, sizeof(rb::SweepStats), cudaMemcpyDeviceToHost, c->stream));
     rb_status st = readCounters(c);
@@ -819,6 +909,42 @@ rb_status rb_read_node_grid(rb_ctx* c, uint32_t node, uint32_t* words) {
     RB_CUDA(c, cudaMemcpy(&g, c->d.grid + node, 4, cudaMemcpyDeviceToHost));
     if (g == kNone) return fail(c, RB_ERR_INVALID_ARG, "node has no grid");
     RB_CUDA(c, cudaMemcpy(words, c->d.arena + (uint64_t)g * 16ull, rb::kGridBytes, cudaMemcpyDeviceToHost));
+    return RB_OK;
+}
+
+rb_status rb_set_profiling(rb_ctx* c, int on) {
+    if (!c) return RB_ERR_INVALID_ARG;
+    c->prof.resolve();
+    c->prof.on = on != 0;
+    return RB_OK;
+}
+
+rb_status rb_read_profile(rb_ctx* c, rb_kernel_profile* out, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (c->stream) RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->prof.resolve();
+    *count = K_NUM;
+    if (!out) return RB_OK;
+    if (capacity < (uint32_t)K_NUM) return fail(c, RB_ERR_CAPACITY, "profile buffer too small");
+    for (int k = 0; k < K_NUM; k++) {
+        std::memset(&out[k], 0, sizeof(out[k]));
+        std::snprintf(out[k].name, sizeof(out[k].name), "%s", kKernelNames[k]);
+        out[k].launches = c->prof.launches[k];
+        out[k].timed_launches = c->prof.timed[k];
+        out[k].total_ms = c->prof.ms[k];
+        out[k].units = c->prof.units[k];
+    }
+    return RB_OK;
+}
+
+rb_status rb_reset_profile(rb_ctx* c) {
+    if (!c) return RB_ERR_INVALID_ARG;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->prof.resolve();
+    for (int k = 0; k < K_NUM; k++) {
+        c->prof.launches[k] = c->prof.timed[k] = c->prof.units[k] = 0;
+        c->prof.ms[k] = 0.0;
+    }
     return RB_OK;
 }
 

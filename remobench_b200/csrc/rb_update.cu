@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict_
                 if (leaf != kNone) d.spillLeaf[j] = leaf;
             }
         }
-        countAt(d, leaf);
+        if (__any_sync(0xFFFFFFFFu, leaf != kNone)) countAt(d, leaf);
     }
 }
 
@@ -286,9 +286,10 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
             r.numChunks = nch;
             // chunks go back to the queue (remolod_octree.cu:349-360)
             const uint32_t owned = d.numPointChunks[node];
-            for (uint32_t j = 0; j < owned; j++) {
-                const uint32_t idx = atomicSub(&c->numAllocatedChunks, 1u) - 1u;
-                if (idx < d.maxPtChunks) d.chunkQueue[idx] = d.tablePool[r.tableOff + j];
+            if (owned) {
+                const uint32_t base0 = atomicSub(&c->numAllocatedChunks, owned) - owned;
+                for (uint32_t j = 0; j < owned; j++)
+                    if (base0 + j < d.maxPtChunks) d.chunkQueue[base0 + j] = d.tablePool[r.tableOff + j];
             }
             d.numPoints[node] = 0;
             d.numPointChunks[node] = 0;
@@ -482,15 +483,26 @@ __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
     const Counters* c = d.ctr;
     if (c->batchStop) return;
     const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nnew; e += gridDim.x * blockDim.x) {
-        const uint32_t slot = d.hashNew[e];
-        const unsigned long long key = d.hashKeys[slot];
-        const uint32_t node = (uint32_t)(key >> 21);
-        const uint32_t vi = (uint32_t)(key & 0x1FFFFFull);
-        const uint32_t g = d.grid[node];
-        atomicOr(gridWordsAt(d, g) + (vi >> 5), 1u << (vi & 31u));
-        d.hashNewNode[e] = node;
-        d.hashNewSlot[e] = atomicAdd(&d.numVoxels[node], 1u);
+    const uint32_t lane = laneId();
+    for (uint32_t base = blockIdx.x * blockDim.x; base < nnew; base += gridDim.x * blockDim.x) {
+        const uint32_t e = base + threadIdx.x;
+        uint32_t node = kNone;
+        if (e < nnew) {
+            const uint32_t slot = d.hashNew[e];
+            const unsigned long long key = d.hashKeys[slot];
+            node = (uint32_t)(key >> 21);
+            const uint32_t vi = (uint32_t)(key & 0x1FFFFFull);
+            atomicOr(gridWordsAt(d, d.grid[node]) + (vi >> 5), 1u << (vi & 31u));
+            d.hashNewNode[e] = node;
+        }
+        // one counter bump per warp and node
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, node);
+        if (node == kNone) continue;
+        const int leader = __ffs(peers) - 1;
+        uint32_t b0 = 0;
+        if ((int)lane == leader) b0 = atomicAdd(&d.numVoxels[node], (uint32_t)__popc(peers));
+        b0 = __shfl_sync(peers, b0, leader);
+        d.hashNewSlot[e] = b0 + __popc(peers & ((1u << lane) - 1u));
     }
 }
 
@@ -546,18 +558,28 @@ __global__ void __launch_bounds__(256) k_alloc_chunks(Dev d) {
             const uint32_t ex = (npts + ppc - 1u) / ppc;
             if (req > ex && ensureTable(d, d.ptTableOff, d.ptTableCap, node, req, ex)) {
                 const uint32_t off = d.ptTableOff[node];
-                for (uint32_t e = ex; e < req; e++) {
-                    const uint32_t idx = atomicAdd(&c->numAllocatedChunks, 1u);
+                const uint32_t extra = req - ex;
+                // logical queue positions [idx0, idx0 + extra): recycled below
+                // poolBefore, fresh from the arena at and above it
+                const uint32_t idx0 = atomicAdd(&c->numAllocatedChunks, extra);
+                const uint32_t firstFresh = idx0 > poolBefore ? idx0 : poolBefore;
+                const uint32_t fresh = idx0 + extra > firstFresh ? idx0 + extra - firstFresh : 0u;
+                uint32_t freshBase = kNone;
+                if (fresh) {
+                    freshBase = arenaAlloc(d, fresh * d.ptChunkUnits);
+                    atomicAdd(&c->numPtChunks, fresh);
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
+                              (unsigned long long)fresh * refAllocSize(kRefChunkBytes));
+                }
+                for (uint32_t e = 0; e < extra; e++) {
+                    const uint32_t idx = idx0 + e;
                     uint32_t phys;
-                    if (idx < poolBefore && idx < d.maxPtChunks) {
-                        phys = d.chunkQueue[idx];
+                    if (idx < poolBefore) {
+                        phys = idx < d.maxPtChunks ? d.chunkQueue[idx] : kNone;
                     } else {
-                        phys = arenaAlloc(d, d.ptChunkUnits);
-                        atomicAdd(&c->numPtChunks, 1u);
-                        atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
-                                  (unsigned long long)refAllocSize(kRefChunkBytes));
+                        phys = freshBase == kNone ? kNone : freshBase + (idx - firstFresh) * d.ptChunkUnits;
                     }
-                    d.tablePool[off + e] = phys;
+                    d.tablePool[off + ex + e] = phys;
                 }
                 d.numPointChunks[node] = req;
             }
@@ -568,15 +590,17 @@ __global__ void __launch_bounds__(256) k_alloc_chunks(Dev d) {
         const uint32_t havev = d.numVoxelChunks[node];
         if (reqv > havev && ensureTable(d, d.vxTableOff, d.vxTableCap, node, reqv, havev)) {
             const uint32_t off = d.vxTableOff[node];
-            for (uint32_t e = havev; e < reqv; e++) {
-                const uint32_t phys = arenaAlloc(d, d.vxChunkUnits);
-                atomicAdd(&c->numVxChunks, 1u);
-                atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
-                          (unsigned long long)refAllocSize(kRefChunkBytes));
-                d.tablePool[off + e] = phys;
-            }
+            const uint32_t extra = reqv - havev;
+            const uint32_t base = arenaAlloc(d, extra * d.vxChunkUnits);
+            atomicAdd(&c->numVxChunks, extra);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
+                      (unsigned long long)extra * refAllocSize(kRefChunkBytes));
+            for (uint32_t e = 0; e < extra; e++)
+                d.tablePool[off + havev + e] = base == kNone ? kNone : base + e * d.vxChunkUnits;
             d.numVoxelChunks[node] = reqv;
         }
+        // every new voxel of this batch is stored by k_vox_store (insertVoxels, :918-938)
+        d.numVoxelsStored[node] = nv;
     }
 }
 
@@ -652,7 +676,6 @@ __global__ void __launch_bounds__(256) k_vox_store(Dev d) {
         v.y = __fadd_rn(mny, __fdiv_rn(__fmul_rn(nodeSize, __fadd_rn((float)py, 0.5f)), 128.0f));
         v.z = __fadd_rn(mnz, __fdiv_rn(__fmul_rn(nodeSize, __fadd_rn((float)pz, 0.5f)), 128.0f));
         v.color = (uint32_t)(val & 0xFFFFFFFFull);
-        atomicAdd(&d.numVoxelsStored[node], 1u);
         if (s < d.numVoxelChunks[node] * ppc) {
             const uint32_t phys = d.tablePool[d.vxTableOff[node] + s / ppc];
             if (phys != kNone) chunkPoints(d, phys)[s % ppc] = v;

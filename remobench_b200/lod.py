@@ -170,6 +170,23 @@ class Context:
         self._ok(capi.lib().rb_read_node_grid(self.h, i, ctypes.c_void_p(g.ctypes.data)))
         return g
 
+    def set_stream(self, stream_handle):
+        self._ok(capi.lib().rb_set_stream(self.h, ctypes.c_void_p(int(stream_handle))))
+
+    def set_profiling(self, on):
+        self._ok(capi.lib().rb_set_profiling(self.h, 1 if on else 0))
+
+    def reset_profile(self):
+        self._ok(capi.lib().rb_reset_profile(self.h))
+
+    def profile(self):
+        n = ctypes.c_uint32()
+        self._ok(capi.lib().rb_read_profile(self.h, None, 0, ctypes.byref(n)))
+        arr = (capi.KernelProfile * n.value)()
+        self._ok(capi.lib().rb_read_profile(self.h, ctypes.cast(arr, ctypes.c_void_p), n.value, ctypes.byref(n)))
+        return {k.name.decode(): {"launches": k.launches, "timed": k.timed_launches, "ms": k.total_ms,
+                                  "units": k.units} for k in arr}
+
     def accums(self):
         n = ctypes.c_uint32()
         self._ok(capi.lib().rb_read_accums(self.h, None, 0, ctypes.byref(n)))

@@ -36,9 +36,9 @@ def test_abi_version_and_status_strings():
     assert lib.rb_status_string(5) == b"ring depth mismatch"
 
 
-STRUCTS = ["rb_config", "rb_cloud_meta", "rb_batch_view", "rb_frame", "rb_build_result", "rb_stats",
+STRUCTS = ["rb_kernel_profile", "rb_config", "rb_cloud_meta", "rb_batch_view", "rb_frame", "rb_build_result", "rb_stats",
            "rb_render_result", "rb_accum_globals", "rb_accum", "rb_node_info", "rb_point"]
-PY = {"rb_config": capi.Config, "rb_cloud_meta": capi.CloudMeta, "rb_batch_view": capi.BatchView,
+PY = {"rb_kernel_profile": capi.KernelProfile, "rb_config": capi.Config, "rb_cloud_meta": capi.CloudMeta, "rb_batch_view": capi.BatchView,
       "rb_frame": capi.Frame, "rb_build_result": capi.BuildResult, "rb_stats": capi.Stats,
       "rb_render_result": capi.RenderResult, "rb_accum_globals": capi.AccumGlobals, "rb_accum": capi.Accum,
       "rb_node_info": capi.NodeInfo}

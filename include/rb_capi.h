@@ -266,6 +266,23 @@ rb_status rb_accumulate(struct rb_ctx* ctx, uint32_t batch_index, rb_accum_globa
 rb_status rb_render(struct rb_ctx* ctx, const rb_frame* frame, uint64_t fb_dev, uint64_t rgba_dev,
                     uint64_t force_large_dev, rb_render_result* out);
 
+/* rb_render without any allocation. No counterpart in the reference: its
+ * render allocates nothing per frame only because the pipeline sized one
+ * scratch buffer up front (RemolodPipeline.cpp:543-557), and its EDL pass runs
+ * inside the same kernel. This entry point is for callers that build the tree
+ * ahead of time but must render where they cannot allocate: a frame callback
+ * with a hard real-time budget that may not take the allocator's lock or risk
+ * an allocation failure mid-frame, or an embedder whose own pool owns all
+ * device memory after start-up. It calls no cudaMalloc/cudaFree; its scratch
+ * (per-node flags, the draw list, three counters) is a static device array of
+ * about 1 MB that every GPU loading this library holds until exit. Limits:
+ * max_nodes <= 262144 and drawlist_capacity <= 131072, else RB_ERR_CAPACITY.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture. Calls share
+ * the array: calls that overlap on the GPU race. Output equals rb_render's. */
+rb_status rb_render_noalloc(struct rb_ctx* ctx, const rb_frame* frame, uint64_t fb_dev, uint64_t rgba_dev,
+                            uint64_t force_large_dev, rb_render_result* out);
+
 /* The flat pipeline (kernels/flat/flat_render.cu:9-76): every point of a
  * resident cloud. */
 rb_status rb_render_flat(struct rb_ctx* ctx, const rb_frame* frame, uint64_t points_dev, uint64_t n,

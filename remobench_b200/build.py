@@ -28,6 +28,7 @@ CUDA_UNITS = {
     "rb_render.cu": ["-fmad=false"],
     "rb_accum.cu": [],
     "rb_capi.cu": [],
+    "rb_noalloc.cu": [],
 }
 
 

@@ -105,6 +105,7 @@ SIGNATURES = {
     "rb_ingest_host": (i32, [_vp, _vp, u64, u32, ctypes.POINTER(BuildResult)]),
     "rb_accumulate": (i32, [_vp, u32, ctypes.POINTER(AccumGlobals)]),
     "rb_render": (i32, [_vp, ctypes.POINTER(Frame), u64, u64, u64, ctypes.POINTER(RenderResult)]),
+    "rb_render_noalloc": (i32, [_vp, ctypes.POINTER(Frame), u64, u64, u64, ctypes.POINTER(RenderResult)]),
     "rb_render_flat": (i32, [_vp, ctypes.POINTER(Frame), u64, u64, u64, u64, ctypes.POINTER(RenderResult)]),
     "rb_read_stats": (i32, [_vp, ctypes.POINTER(Stats)]),
     "rb_read_nodes": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),

@@ -964,3 +964,36 @@ rb_status rb_read_accums(rb_ctx* c, rb_accum* out, uint32_t capacity, uint32_t* 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ access
+#include "rb_ctx_access.h"
+
+namespace rb {
+
+bool ctxRenderAccess(rb_ctx* c, CtxRenderAccess* out) {
+    if (!c || !out) return false;
+    out->d = c->d;
+    out->stream = c->stream;
+    out->device = c->device;
+    out->numSMs = c->numSMs;
+    out->pipeline = c->cfg.pipeline;
+    out->maxNodes = c->cfg.max_nodes;
+    out->drawlistCapacity = c->cfg.drawlist_capacity;
+    out->allocated = c->allocated;
+    out->hostRs = c->hostRs;
+    out->evStart = c->evStart;
+    out->evStop = c->evStop;
+    return true;
+}
+
+void ctxSetError(rb_ctx* c, const char* msg) {
+    if (c) c->err = msg ? msg : "";
+}
+
+void ctxNoteVisible(rb_ctx* c, uint32_t nodes, uint64_t samples) {
+    if (!c) return;
+    c->lastVisibleNodes = nodes;
+    c->lastVisibleSamples = samples;
+}
+
+}  // namespace rb

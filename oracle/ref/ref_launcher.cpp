@@ -82,6 +82,8 @@ int gridFor(Handle* h, CUfunction f, int block, int smFactor) {
 
 extern "C" {
 
+int ref_accumulate(void* hp, void* globalsOut);
+
 const char* ref_last_error(void* hp) { return hp ? static_cast<Handle*>(hp)->err.c_str() : "null"; }
 
 int ref_open(const char* cubinDir, const char* variant, void** out) {
@@ -185,6 +187,49 @@ int ref_construct(void* hp, uint32_t* batchletIndex) {
     h->batchesConsumed = s.batchletIndex;
     *batchletIndex = s.batchletIndex;
     return 0;
+}
+
+// ref_construct with the launch bracketed by CUDA events (GpuScope,
+// include/remo/GpuProfiler.h:143-158); *ms receives the kernel's device time.
+int ref_construct_timed(void* hp, uint32_t* batchletIndex, float* ms) {
+    Handle* h = static_cast<Handle*>(hp);
+    CK(h, cuCtxSetCurrent(h->ctx));
+    CUevent a, b;
+    CK(h, cuEventCreate(&a, CU_EVENT_DEFAULT));
+    CK(h, cuEventCreate(&b, CU_EVENT_DEFAULT));
+    Uniforms u = makeUniforms(h);
+    void* args[] = {&u,          &h->ring,       &h->momentary, &h->persistent, &h->nodes, &h->stats,
+                    &h->frameStart, &h->cudaPrint, &h->uploaded,   &h->sizes,      &h->timeline};
+    const int grid = gridFor(h, h->fConstruct, 256, 1);
+    CK(h, cuEventRecord(a, 0));
+    CK(h, cuLaunchCooperativeKernel(h->fConstruct, (unsigned)grid, 1, 1, 256, 1, 1, 0, 0, args));
+    CK(h, cuEventRecord(b, 0));
+    CK(h, cuEventSynchronize(b));
+    CK(h, cuEventElapsedTime(ms, a, b));
+    cuEventDestroy(a);
+    cuEventDestroy(b);
+    Stats s;
+    CK(h, cuMemcpyDtoH(&s, h->stats, sizeof(Stats)));
+    h->batchesConsumed = s.batchletIndex;
+    *batchletIndex = s.batchletIndex;
+    return 0;
+}
+
+// ref_accumulate's two launches timed the same way.
+int ref_accumulate_timed(void* hp, void* globalsOut, float* ms) {
+    Handle* h = static_cast<Handle*>(hp);
+    CK(h, cuCtxSetCurrent(h->ctx));
+    CUevent a, b;
+    CK(h, cuEventCreate(&a, CU_EVENT_DEFAULT));
+    CK(h, cuEventCreate(&b, CU_EVENT_DEFAULT));
+    CK(h, cuEventRecord(a, 0));
+    const int rc = ref_accumulate(hp, globalsOut);
+    CK(h, cuEventRecord(b, 0));
+    CK(h, cuEventSynchronize(b));
+    CK(h, cuEventElapsedTime(ms, a, b));
+    cuEventDestroy(a);
+    cuEventDestroy(b);
+    return rc;
 }
 
 // runAccumulator (RemolodPipeline.cpp:242-294).

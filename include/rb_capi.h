@@ -300,6 +300,54 @@ rb_status rb_read_node_voxels(struct rb_ctx* ctx, uint32_t node, rb_point* vox, 
 rb_status rb_read_node_grid(struct rb_ctx* ctx, uint32_t node, uint32_t* words65536);
 rb_status rb_read_accums(struct rb_ctx* ctx, rb_accum* out, uint32_t capacity, uint32_t* count);
 
+/* Analysis (no reference kernel; wiki/02_KernelPipeline.md:204-224 describes
+ * it): exact roll-up of the leaf sums, centred covariance, 3x3 eigen-solve,
+ * surface variation and planarity x screen coverage, per-frame priority queue. */
+typedef struct rb_analysis_params {
+    uint32_t min_points;       /* nodes with fewer points score 0 (16) */
+    uint32_t closure_margin;   /* batches without new points before a node is closed (8) */
+    uint32_t frontier_only;    /* queue only nodes Refinement can open (1) */
+    uint32_t queue_capacity;   /* top-K kept (<= 16384) */
+    float pixel_budget;        /* the LOD cut's budget, to find the frontier (128) */
+    uint32_t pad;
+} rb_analysis_params;
+
+typedef struct rb_analysis_result {
+    uint32_t queue_length;
+    uint32_t eligible;         /* nodes with a positive score that may enter the queue */
+    uint32_t fp64_branch;      /* eigen-solves that took the FP64 near-degenerate branch */
+    uint32_t overflow;         /* more tied candidates than the queue sort holds */
+    float device_ms;
+    uint32_t pad;
+} rb_analysis_result;
+
+typedef struct rb_node_analysis {
+    float eig[3];              /* descending, units of (node size)^2 */
+    float normal[3];           /* eigenvector of eig[2] */
+    float surface_variation;   /* eig[2] / sum */
+    float planarity;           /* (eig[1] - eig[2]) / eig[0] */
+    float coverage;            /* fraction of the frame under the node's projected box */
+    float score;               /* surface variation x coverage */
+    uint64_t count;            /* points in the subtree */
+    uint32_t last_touched;     /* newest batch index that added points to the subtree */
+    uint32_t closed;
+    uint32_t flags;            /* 1: FP64 branch, 2: large, 4: frontier */
+    uint32_t pad;
+} rb_node_analysis;
+
+rb_status rb_analyze(struct rb_ctx* ctx, const rb_frame* frame, const rb_analysis_params* params,
+                     rb_analysis_result* out);
+rb_status rb_read_analysis(struct rb_ctx* ctx, rb_node_analysis* out, uint32_t capacity, uint32_t* count);
+rb_status rb_read_queue(struct rb_ctx* ctx, uint32_t* node_ids, uint32_t capacity, uint32_t* count);
+/* Exact rolled sums per node: n, s1[3], s2 as (lo, hi) x 6 -- 16 uint64 per node. */
+rb_status rb_read_rollup(struct rb_ctx* ctx, uint64_t* out16, uint32_t capacity, uint32_t* count);
+
+/* Refinement, minimal budgeted form (wiki/02_KernelPipeline.md:228-243 lists
+ * the passes; this is the budget consumer): the first `budget` nodes of the
+ * last Analysis queue are written as 1 into the node mask at mask_dev (one
+ * byte per node), which rb_render takes as force_large_dev. */
+rb_status rb_refine(struct rb_ctx* ctx, uint32_t budget, uint64_t mask_dev);
+
 /* Kernel timing (see rb_kernel_profile). */
 rb_status rb_set_profiling(struct rb_ctx* ctx, int on);
 rb_status rb_read_profile(struct rb_ctx* ctx, rb_kernel_profile* out, uint32_t capacity, uint32_t* count);

@@ -123,6 +123,12 @@ class AnalysisNode(ctypes.Structure):
     ]
 
 
+class AnalysisParams(ctypes.Structure):
+    _fields_ = [("min_points", ctypes.c_uint32), ("closure_margin", ctypes.c_uint32),
+                ("current_batch", ctypes.c_uint32), ("frontier_only", ctypes.c_uint32),
+                ("pixel_budget", ctypes.c_float), ("pad", ctypes.c_uint32)]
+
+
 class Frame(ctypes.Structure):
     _fields_ = [
         ("width", ctypes.c_float),
@@ -181,6 +187,8 @@ def lib():
         L.or_analyze_fp64.argtypes = [vp, vp]
         L.or_sym3_eig_jacobi.argtypes = [vp, vp, vp]
         L.or_render.argtypes = [vp, ctypes.POINTER(Frame), vp, ctypes.POINTER(RenderResult), vp]
+        L.or_rolled_sums.argtypes = [vp, vp, vp]
+        L.or_analysis_scores.argtypes = [vp, ctypes.POINTER(Frame), ctypes.POINTER(AnalysisParams), vp, vp, vp, vp, vp]
         L.or_render_flat.argtypes = [vp, u64, ctypes.POINTER(Frame), vp]
         L.or_edl.argtypes = [vp, u32, u32, ctypes.c_float]
         _lib = L
@@ -304,6 +312,23 @@ class Tree:
         arr = (AnalysisNode * max(nn, 1))()
         lib().or_analyze_fp64(self.h, ctypes.cast(arr, ctypes.c_void_p))
         return arr
+
+    def rolled_sums(self):
+        nn = self.num_nodes()
+        out = np.zeros((nn, 16), dtype=np.uint64)
+        lt = np.zeros(nn, dtype=np.uint32)
+        lib().or_rolled_sums(self.h, _ptr(out), _ptr(lt))
+        return out, lt
+
+    def analysis_scores(self, frame, params, analysis):
+        nn = self.num_nodes()
+        cov = np.zeros(nn, dtype=np.float32)
+        flags = np.zeros(nn, dtype=np.uint32)
+        closed = np.zeros(nn, dtype=np.uint32)
+        score = np.zeros(nn, dtype=np.float64)
+        lib().or_analysis_scores(self.h, ctypes.byref(frame), ctypes.byref(params), ctypes.cast(analysis, ctypes.c_void_p),
+                                 _ptr(cov), _ptr(flags), _ptr(closed), _ptr(score))
+        return cov, flags, closed, score
 
     def render(self, frame, item_nodes_cap=0):
         w, h = int(frame.width), int(frame.height)

@@ -810,6 +810,37 @@ void or_sym3_eig_jacobi(const double a_in[6], double eig[3], double vmin[3]) {
     for (int k = 0; k < 3; k++) vmin[k] = v[k][ord[2]];
 }
 
+void or_rolled_sums(const or_tree* t, uint64_t* out16, uint32_t* last_touched) {
+    const uint32_t nn = t->num_nodes;
+    roll* all = (roll*)calloc(nn ? nn : 1, sizeof(roll));
+    uint32_t* lt = (uint32_t*)calloc(nn ? nn : 1, sizeof(uint32_t));
+    if (!all || !lt) abort();
+    for (uint32_t k = nn; k-- > 0;) {
+        roll_node(t, k, &all[k], all);
+        const onode* n = &t->nodes[k];
+        if (is_leaf(n)) {
+            lt[k] = n->ai.count ? n->ai.last_touched_batch : 0u;
+        } else {
+            uint32_t m = 0;
+            for (int c = 0; c < 8; c++)
+                if (n->child[c] >= 0 && all[n->child[c]].n > 0 && lt[n->child[c]] > m) m = lt[n->child[c]];
+            lt[k] = m;
+        }
+    }
+    for (uint32_t i = 0; i < nn; i++) {
+        uint64_t* o = out16 + (size_t)i * 16;
+        o[0] = (uint64_t)all[i].n;
+        for (int a = 0; a < 3; a++) o[1 + a] = (uint64_t)all[i].s1[a];
+        for (int k = 0; k < 6; k++) {
+            o[4 + 2 * k] = (uint64_t)all[i].s2[k];
+            o[4 + 2 * k + 1] = (uint64_t)(all[i].s2[k] >> 64);
+        }
+        if (last_touched) last_touched[i] = lt[i];
+    }
+    free(all);
+    free(lt);
+}
+
 void or_analyze_fp64(const or_tree* t, or_analysis_node* out) {
     const uint32_t nn = t->num_nodes;
     roll* all = (roll*)calloc(nn ? nn : 1, sizeof(roll));
@@ -836,6 +867,49 @@ void or_analyze_fp64(const or_tree* t, or_analysis_node* out) {
         o->planarity = o->eig[0] > 0.0 ? (o->eig[1] - o->eig[2]) / o->eig[0] : 0.0;
     }
     free(all);
+}
+
+static void box_extent(const or_frame* f, float cube, uint32_t level, uint32_t X, uint32_t Y, uint32_t Z,
+                       float ext[4], int* any);
+
+void or_analysis_scores(const or_tree* t, const or_frame* f, const or_analysis_params* p,
+                        const or_analysis_node* eig, float* coverage, uint32_t* flags, uint32_t* closed,
+                        double* score) {
+    const uint32_t nn = t->num_nodes;
+    uint32_t* lt = (uint32_t*)calloc(nn ? nn : 1, sizeof(uint32_t));
+    uint64_t* sums = (uint64_t*)calloc((size_t)(nn ? nn : 1) * 16, sizeof(uint64_t));
+    if (!lt || !sums) abort();
+    or_rolled_sums(t, sums, lt);
+    float sx = f->box_max[0] - f->box_min[0], sy = f->box_max[1] - f->box_min[1], sz = f->box_max[2] - f->box_min[2];
+    float cube = fmaxf(fmaxf(sx, sy), sz);
+    for (uint32_t i = 0; i < nn; i++) {
+        const onode* n = &t->nodes[i];
+        float e0[4], e1[4];
+        int a0 = 0, a1 = 0;
+        box_extent(f, cube, n->level, n->X, n->Y, n->Z, e0, &a0);
+        if (n->level > 0) box_extent(f, cube, n->level - 1, n->X >> 1, n->Y >> 1, n->Z >> 1, e1, &a1);
+        float cov = 0.0f;
+        int large = 0, parent_large = n->level == 0;
+        if (a0) {
+            float x0 = fmaxf(e0[0], 0.0f), x1 = fminf(e0[1], f->width);
+            float y0 = fmaxf(e0[2], 0.0f), y1 = fminf(e0[3], f->height);
+            if (x1 > x0 && y1 > y0) cov = (x1 - x0) * (y1 - y0) / (f->width * f->height);
+            large = (e0[1] - e0[0]) > p->pixel_budget || (e0[3] - e0[2]) > p->pixel_budget;
+        }
+        if (n->level > 0 && a1) parent_large = (e1[1] - e1[0]) > p->pixel_budget || (e1[3] - e1[2]) > p->pixel_budget;
+        uint32_t fl = 0;
+        if (large) fl |= 2u;
+        if (!is_leaf(n) && !large && parent_large) fl |= 4u;
+        coverage[i] = cov;
+        flags[i] = fl;
+        uint64_t cnt = sums[(size_t)i * 16];
+        closed[i] = (p->current_batch >= lt[i] + p->closure_margin && cnt > 0) ? 1u : 0u;
+        double sc = eig[i].surface_variation * (double)cov;
+        if (cnt < p->min_points) sc = 0.0;
+        score[i] = sc;
+    }
+    free(lt);
+    free(sums);
 }
 
 /* ------------------------------------------------------------ Rasterize */
@@ -893,6 +967,37 @@ static int frustum_box(const plane pl[6], const float mn[3], const float mx[3]) 
         if (pl[i].nx * px + pl[i].ny * py + pl[i].nz * pz + pl[i].d < 0.0f) return 0;
     }
     return 1;
+}
+
+/* the node's projected box (projectedExtent, remolod_render.cu:40-70) in the
+ * frozen transform: [minX, maxX, minY, maxY] */
+static void box_extent(const or_frame* f, float cube, uint32_t level, uint32_t X, uint32_t Y, uint32_t Z,
+                       float ext[4], int* any) {
+    float s = cube / ldexpf(1.0f, (int)level);
+    float mn[3] = {f->box_min[0] + (float)X * s, f->box_min[1] + (float)Y * s, f->box_min[2] + (float)Z * s};
+    float minX = 1e30f, minY = 1e30f, maxX = -1e30f, maxY = -1e30f;
+    *any = 0;
+    for (int c = 0; c < 8; c++) {
+        float x = (c & 1) ? mn[0] + s : mn[0];
+        float y = (c & 2) ? mn[1] + s : mn[1];
+        float z = (c & 4) ? mn[2] + s : mn[2];
+        const float* m = f->transform_frozen;
+        float cx = m[0] * x + m[1] * y + m[2] * z + m[3];
+        float cy = m[4] * x + m[5] * y + m[6] * z + m[7];
+        float cw = m[12] * x + m[13] * y + m[14] * z + m[15];
+        if (cw <= 0.0f) continue;
+        float iw = 1.0f / cw;
+        float px = (cx * iw * 0.5f + 0.5f) * f->width, py = (cy * iw * 0.5f + 0.5f) * f->height;
+        minX = fminf(minX, px);
+        maxX = fmaxf(maxX, px);
+        minY = fminf(minY, py);
+        maxY = fmaxf(maxY, py);
+        *any = 1;
+    }
+    ext[0] = minX;
+    ext[1] = maxX;
+    ext[2] = minY;
+    ext[3] = maxY;
 }
 
 /* nodeBounds (remolod_render.cu:30-38) */

@@ -15,8 +15,9 @@
  * Parity pinning: the reference ships no tests, fixtures or golden vectors for
  * this path (its only structural pins are on lidar files that are not
  * distributed), so this restatement is pinned against the reference's own
- * invariants and against hand-computed cases in tests/; it is
- * "parity unpinned" with respect to outputs of the reference itself.
+ * invariants, against hand-computed cases, and against outputs of the
+ * reference's own kernels run on a B200 (tests/golden/ref_config1_*.npz, made
+ * by tests/golden/make_ref_fixtures.py; checked in tests/test_ref_pin.py).
  */
 #ifndef RB_ORACLE_H
 #define RB_ORACLE_H
@@ -81,6 +82,7 @@ typedef struct or_stats {
 #define OR_OVERFLOW_SPILLING 4u  /* more than 100k spilling nodes in an iteration */
 
 typedef struct or_tree or_tree;
+typedef struct or_frame or_frame;
 
 or_tree* or_create(const or_config* cfg);
 void or_destroy(or_tree* t);
@@ -166,9 +168,31 @@ void or_analyze_fp64(const or_tree* t, or_analysis_node* out);
 /* Eigenvalues of a symmetric 3x3 (a00 a01 a02 a11 a12 a22) by cyclic Jacobi. */
 void or_sym3_eig_jacobi(const double a[6], double eig[3], double vmin[3]);
 
+/* The exact rolled sums behind or_analyze_fp64: per node 16 uint64 (n, s1[3],
+ * s2 as lo/hi pairs xx xy xz yy yz zz) and the newest batch that added points
+ * to the subtree (accumulators' last_touched_batch, rolled up by max). */
+void or_rolled_sums(const or_tree* t, uint64_t* out16, uint32_t* last_touched);
+
+typedef struct or_analysis_params {
+    uint32_t min_points;
+    uint32_t closure_margin;
+    uint32_t current_batch;
+    uint32_t frontier_only;
+    float pixel_budget;
+    uint32_t pad;
+} or_analysis_params;
+
+/* Screen coverage, flags (2: large, 4: frontier), closure and score
+ * (surface variation x coverage, 0 below min_points) per node, from
+ * or_analyze_fp64's eigenvalues; the projected extents use the LOD cut's float
+ * arithmetic (remolod_render.cu:40-70). */
+void or_analysis_scores(const or_tree* t, const or_frame* f, const or_analysis_params* p,
+                        const or_analysis_node* eig, float* coverage, uint32_t* flags, uint32_t* closed,
+                        double* score);
+
 /* ------------------------------------------------------------ Rasterize */
 
-typedef struct or_frame {
+struct or_frame {
     float width, height;
     float transform[16];         /* row-major clip = M * (x, y, z, 1) */
     float transform_frozen[16];  /* LOD-selection transform */
@@ -178,7 +202,7 @@ typedef struct or_frame {
     uint32_t drawlist_capacity;  /* 131072 (remolod_render.cu:22) */
     /* optional: nodes forced large (Refinement); NULL or num_nodes bytes */
     const uint8_t* force_large;
-} or_frame;
+};
 
 typedef struct or_render_result {
     uint32_t draw_items;

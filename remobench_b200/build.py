@@ -29,6 +29,7 @@ CUDA_UNITS = {
     "rb_accum.cu": [],
     "rb_capi.cu": [],
     "rb_noalloc.cu": [],
+    "rb_analysis.cu": ["-fmad=false"],
 }
 
 
@@ -63,8 +64,13 @@ def build_cuda(force=False):
     for unit, extra in CUDA_UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(BUILD, unit + ".o")
-        if force or _stale(obj, [src] + hdrs):
-            _run([nvcc] + ARCH + NVCC_FLAGS + extra + ["-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj])
+        cmd = [nvcc] + ARCH + NVCC_FLAGS + extra + ["-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+        stamp = obj + ".cmd"
+        same_cmd = os.path.exists(stamp) and open(stamp).read() == " ".join(cmd)
+        if force or not same_cmd or _stale(obj, [src] + hdrs):
+            _run(cmd)
+            with open(stamp, "w") as f:
+                f.write(" ".join(cmd))
         objs.append(obj)
     out = os.path.join(LIB, "librb_cuda.so")
     if force or _stale(out, objs):

@@ -83,6 +83,22 @@ class NodeInfo(ctypes.Structure):
                 ("num_voxel_chunks", u32), ("is_leaf", u32)]
 
 
+class AnalysisParams(ctypes.Structure):
+    _fields_ = [("min_points", u32), ("closure_margin", u32), ("frontier_only", u32), ("queue_capacity", u32),
+                ("pixel_budget", f32), ("pad", u32)]
+
+
+class AnalysisResult(ctypes.Structure):
+    _fields_ = [("queue_length", u32), ("eligible", u32), ("fp64_branch", u32), ("overflow", u32),
+                ("device_ms", f32), ("pad", u32)]
+
+
+class NodeAnalysis(ctypes.Structure):
+    _fields_ = [("eig", f32 * 3), ("normal", f32 * 3), ("surface_variation", f32), ("planarity", f32),
+                ("coverage", f32), ("score", f32), ("count", u64), ("last_touched", u32), ("closed", u32),
+                ("flags", u32), ("pad", u32)]
+
+
 class KernelProfile(ctypes.Structure):
     _fields_ = [("name", ctypes.c_char * 32), ("launches", u64), ("timed_launches", u64),
                 ("total_ms", ctypes.c_double), ("units", u64)]
@@ -113,6 +129,11 @@ SIGNATURES = {
     "rb_read_node_voxels": (i32, [_vp, u32, _vp, u32, ctypes.POINTER(u32)]),
     "rb_read_node_grid": (i32, [_vp, u32, _vp]),
     "rb_read_accums": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
+    "rb_analyze": (i32, [_vp, ctypes.POINTER(Frame), ctypes.POINTER(AnalysisParams), ctypes.POINTER(AnalysisResult)]),
+    "rb_read_analysis": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
+    "rb_read_queue": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
+    "rb_read_rollup": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
+    "rb_refine": (i32, [_vp, u32, u64]),
     "rb_set_profiling": (i32, [_vp, ctypes.c_int]),
     "rb_read_profile": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_reset_profile": (i32, [_vp]),

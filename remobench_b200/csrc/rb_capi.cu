@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/rb_capi.h"
+#include "rb_analysis.h"
 #include "rb_kernels.h"
 #include "rb_state.h"
 
@@ -23,13 +24,14 @@ enum KernelId : int {
     K_BUILD_BEGIN, K_BATCH_BEGIN, K_COUNT_FIRST, K_SPLIT, K_SPILL_COPY, K_RECOUNT, K_VOX_SAMPLE,
     K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END, K_ACCUMULATE, K_ACCUM_VERIFY,
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
-    K_RESOLVE, K_NUM
+    K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
     "k_vox_sample", "k_vox_commit", "k_alloc_chunks", "k_insert", "k_vox_store", "k_batch_end",
     "k_accumulate", "k_accum_verify", "k_sweep", "k_reset_root", "k_fb_clear", "k_node_flags",
-    "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve"};
+    "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve", "k_roll_level", "k_analyze",
+    "k_queue", "k_refine"};
 
 struct Profiler {
     bool on = false;
@@ -99,6 +101,16 @@ struct rb_ctx {
     rb::RenderScratch* rs = nullptr;
     unsigned long long* fbTmp = nullptr;
     uint64_t fbTmpPixels = 0;
+    // analysis
+    rb::RollSum* roll = nullptr;
+    rb::NodeAnalysis* analysis = nullptr;
+    unsigned long long* akeys = nullptr;
+    uint32_t* ahist = nullptr;
+    unsigned long long* acand = nullptr;
+    uint32_t* aqueue = nullptr;
+    rb::AnalysisCounters* actr = nullptr;
+    rb::AnalysisCounters* hostActr = nullptr;
+    bool analyzed = false;
     // host-ingest ring
     rb::Point* ingestRing = nullptr;
     uint32_t ingestSlots = 0;
@@ -141,6 +153,8 @@ rb_status devAlloc(rb_ctx* c, T** p, uint64_t count, const char* what) {
     *p = static_cast<T*>(q);
     return RB_OK;
 }
+
+constexpr uint32_t kQueueSortCap = 16384;
 
 uint32_t nextPow2(uint64_t v) {
     uint64_t m = 1;
@@ -308,6 +322,9 @@ void rb_release(rb_ctx* c) {
     if (c->hostSweep) cudaFreeHost(c->hostSweep);
     if (c->hostAccum) cudaFreeHost(c->hostAccum);
     if (c->hostRs) cudaFreeHost(c->hostRs);
+    if (c->hostActr) cudaFreeHost(c->hostActr);
+    c->hostActr = nullptr;
+    c->analyzed = false;
     c->hostCtr = nullptr;
     c->hostSweep = nullptr;
     c->hostAccum = nullptr;
@@ -468,6 +485,13 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(c->large, N, "large flags");
     ALLOC(c->items, std::max<uint32_t>(cfg.drawlist_capacity, 1), "draw list");
     ALLOC(c->rs, 1, "render scratch");
+    ALLOC(c->roll, N, "rolled sums");
+    ALLOC(c->analysis, N, "node analysis");
+    ALLOC(c->akeys, N, "queue keys");
+    ALLOC(c->ahist, 65536, "queue histogram");
+    ALLOC(c->acand, kQueueSortCap, "queue candidates");
+    ALLOC(c->aqueue, kQueueSortCap, "queue");
+    ALLOC(c->actr, 1, "analysis counters");
     c->ingestSlots = 3;
     ALLOC(c->ingestRing, (uint64_t)c->ingestSlots * cfg.slot_capacity, "ingest ring");
 #undef ALLOC
@@ -480,6 +504,8 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     RB_CUDA(c, cudaMallocHost(&c->hostSweep, sizeof(rb::SweepStats)));
     RB_CUDA(c, cudaMallocHost(&c->hostAccum, sizeof(rb::AccumGlobals)));
     RB_CUDA(c, cudaMallocHost(&c->hostRs, sizeof(rb::RenderScratch)));
+    RB_CUDA(c, cudaMallocHost(&c->hostActr, sizeof(rb::AnalysisCounters)));
+    RB_CUDA(c, rb::configureQueueSort(kQueueSortCap));
     for (uint32_t i = 0; i < c->ingestSlots; i++) {
         RB_CUDA(c, cudaEventCreateWithFlags(&c->slotFree[i], cudaEventDisableTiming));
         RB_CUDA(c, cudaEventCreateWithFlags(&c->slotFull[i], cudaEventDisableTiming));
@@ -909,6 +935,107 @@ rb_status rb_read_node_grid(rb_ctx* c, uint32_t node, uint32_t* words) {
     RB_CUDA(c, cudaMemcpy(&g, c->d.grid + node, 4, cudaMemcpyDeviceToHost));
     if (g == kNone) return fail(c, RB_ERR_INVALID_ARG, "node has no grid");
     RB_CUDA(c, cudaMemcpy(words, c->d.arena + (uint64_t)g * 16ull, rb::kGridBytes, cudaMemcpyDeviceToHost));
+    return RB_OK;
+}
+
+rb_status rb_analyze(rb_ctx* c, const rb_frame* f, const rb_analysis_params* p, rb_analysis_result* out) {
+    if (!c || !f || !p) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree to analyse");
+    if (p->queue_capacity == 0 || p->queue_capacity > kQueueSortCap)
+        return fail(c, RB_ERR_CAPACITY, "queue_capacity must be in [1, 16384]");
+    if (!(f->width >= 1.0f && f->height >= 1.0f)) return fail(c, RB_ERR_INVALID_ARG, "empty frame");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const int grid = c->numSMs * 4;
+    rb::AnalysisParams ap;
+    ap.minPoints = p->min_points;
+    ap.closureMargin = p->closure_margin;
+    ap.currentBatch = c->batchesConsumed;
+    ap.frontierOnly = p->frontier_only;
+    ap.pixelBudget = p->pixel_budget;
+    ap.pad = 0;
+    const rb::Frame fr = toFrame(f);
+    RB_CUDA(c, cudaEventRecord(c->evStart, s));
+    RB_CUDA(c, cudaMemsetAsync(c->ahist, 0, 65536 * 4, s));
+    RB_CUDA(c, cudaMemsetAsync(c->actr, 0, sizeof(rb::AnalysisCounters), s));
+    for (int L = rb::kMaxDepth; L >= 0; L--)
+        LAUNCH(c, K_ROLL, 0, rb::launchRollLevel(c->d, c->roll, (uint32_t)L, grid, s));
+    LAUNCH(c, K_ANALYZE, 0, rb::launchAnalyze(c->d, c->roll, c->analysis, c->akeys, ap, fr, c->actr, grid, s));
+    LAUNCH(c, K_QUEUE, 0, rb::launchQueue(c->d, c->akeys, c->ahist, c->acand, kQueueSortCap, p->queue_capacity,
+                                          c->aqueue, c->actr, grid, s));
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaEventRecord(c->evStop, s));
+    RB_CUDA(c, cudaMemcpyAsync(c->hostActr, c->actr, sizeof(rb::AnalysisCounters), cudaMemcpyDeviceToHost, s));
+    RB_CUDA(c, cudaStreamSynchronize(s));
+    c->analyzed = true;
+    if (out) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, c->evStart, c->evStop);
+        out->queue_length = c->hostActr->queueLength;
+        out->eligible = c->hostActr->eligible;
+        out->fp64_branch = c->hostActr->fp64Branch;
+        out->overflow = c->hostActr->overflow;
+        out->device_ms = ms;
+        out->pad = 0;
+    }
+    return RB_OK;
+}
+
+static rb_status copyOut(rb_ctx* c, void* out, const void* src, size_t elem, uint32_t capacity, uint32_t* count,
+                         uint32_t n) {
+    *count = n;
+    if (!out) return RB_OK;
+    if (capacity < n) return fail(c, RB_ERR_CAPACITY, "output buffer too small");
+    RB_CUDA(c, cudaMemcpy(out, src, (size_t)n * elem, cudaMemcpyDeviceToHost));
+    return RB_OK;
+}
+
+rb_status rb_read_analysis(rb_ctx* c, rb_node_analysis* out, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (!c->analyzed) return fail(c, RB_ERR_STATE, "read before rb_analyze");
+    static_assert(sizeof(rb_node_analysis) == sizeof(rb::NodeAnalysis), "analysis layout");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    return copyOut(c, out, c->analysis, sizeof(rb_node_analysis), capacity, count, c->hostCtr->numNodes);
+}
+
+rb_status rb_read_queue(rb_ctx* c, uint32_t* ids, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (!c->analyzed) return fail(c, RB_ERR_STATE, "read before rb_analyze");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    return copyOut(c, ids, c->aqueue, 4, capacity, count, c->hostActr->queueLength);
+}
+
+rb_status rb_read_rollup(rb_ctx* c, uint64_t* out16, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (!c->analyzed) return fail(c, RB_ERR_STATE, "read before rb_analyze");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    const uint32_t nn = c->hostCtr->numNodes;
+    *count = nn;
+    if (!out16) return RB_OK;
+    if (capacity < nn) return fail(c, RB_ERR_CAPACITY, "output buffer too small");
+    std::vector<rb::RollSum> tmp(nn);
+    RB_CUDA(c, cudaMemcpy(tmp.data(), c->roll, (size_t)nn * sizeof(rb::RollSum), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < nn; i++) {
+        uint64_t* o = out16 + (size_t)i * 16;
+        o[0] = tmp[i].n;
+        for (int k = 0; k < 3; k++) o[1 + k] = tmp[i].s1[k];
+        for (int k = 0; k < 12; k++) o[4 + k] = tmp[i].s2[k];
+    }
+    return RB_OK;
+}
+
+rb_status rb_refine(rb_ctx* c, uint32_t budget, uint64_t maskDev) {
+    if (!c || !maskDev) return RB_ERR_INVALID_ARG;
+    if (!c->analyzed) return fail(c, RB_ERR_STATE, "refine before rb_analyze");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    LAUNCH(c, K_REFINE, budget, rb::launchRefineMask(c->d, c->aqueue, c->actr, budget,
+                                                     reinterpret_cast<uint8_t*>(maskDev), c->numSMs * 2, c->stream));
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
     return RB_OK;
 }
 

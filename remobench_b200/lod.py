@@ -15,6 +15,9 @@ POINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("color", "<u4
 NODE_DTYPE = np.dtype([("child", "<i4", 8), ("counter", "<u4"), ("num_points", "<u4"), ("level", "<u4"),
                        ("X", "<u4"), ("Y", "<u4"), ("Z", "<u4"), ("has_grid", "<u4"), ("num_voxels", "<u4"),
                        ("num_point_chunks", "<u4"), ("num_voxel_chunks", "<u4"), ("is_leaf", "<u4")])
+ANALYSIS_DTYPE = np.dtype([("eig", "<f4", 3), ("normal", "<f4", 3), ("surface_variation", "<f4"),
+                           ("planarity", "<f4"), ("coverage", "<f4"), ("score", "<f4"), ("count", "<u8"),
+                           ("last_touched", "<u4"), ("closed", "<u4"), ("flags", "<u4"), ("pad", "<u4")])
 ACCUM_DTYPE = np.dtype([("s1", "<u8", 3), ("s2_lo", "<u8", 6), ("s2_hi", "<u8", 6), ("c1", "<u8", 3),
                         ("c2", "<u8", 3), ("count", "<u4"), ("last_touched_batch", "<u4"), ("state", "<u4"),
                         ("pad", "<u4")])
@@ -169,6 +172,43 @@ class Context:
         g = np.zeros(65536, dtype=np.uint32)
         self._ok(capi.lib().rb_read_node_grid(self.h, i, ctypes.c_void_p(g.ctypes.data)))
         return g
+
+    def analyze(self, frame, min_points=16, closure_margin=8, frontier_only=True, queue_capacity=4096,
+                pixel_budget=None):
+        p = capi.AnalysisParams()
+        p.min_points = int(min_points)
+        p.closure_margin = int(closure_margin)
+        p.frontier_only = 1 if frontier_only else 0
+        p.queue_capacity = int(queue_capacity)
+        p.pixel_budget = float(frame.lod_pixel_budget if pixel_budget is None else pixel_budget)
+        r = capi.AnalysisResult()
+        self._ok(capi.lib().rb_analyze(self.h, ctypes.byref(frame), ctypes.byref(p), ctypes.byref(r)))
+        return r
+
+    def analysis(self):
+        n = ctypes.c_uint32()
+        self._ok(capi.lib().rb_read_analysis(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=ANALYSIS_DTYPE)
+        self._ok(capi.lib().rb_read_analysis(self.h, ctypes.c_void_p(out.ctypes.data), n.value, ctypes.byref(n)))
+        return out
+
+    def queue(self):
+        n = ctypes.c_uint32()
+        self._ok(capi.lib().rb_read_queue(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=np.uint32)
+        if n.value:
+            self._ok(capi.lib().rb_read_queue(self.h, ctypes.c_void_p(out.ctypes.data), n.value, ctypes.byref(n)))
+        return out
+
+    def rollup(self):
+        n = ctypes.c_uint32()
+        self._ok(capi.lib().rb_read_rollup(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 16), dtype=np.uint64)
+        self._ok(capi.lib().rb_read_rollup(self.h, ctypes.c_void_p(out.ctypes.data), n.value, ctypes.byref(n)))
+        return out
+
+    def refine(self, budget, mask):
+        self._ok(capi.lib().rb_refine(self.h, int(budget), mask.data_ptr()))
 
     def set_stream(self, stream_handle):
         self._ok(capi.lib().rb_set_stream(self.h, ctypes.c_void_p(int(stream_handle))))

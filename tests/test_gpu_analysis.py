@@ -1,0 +1,128 @@
+"""Analysis on the B200 against the FP64 CPU oracle: exact roll-up, eigenvalues
+within a stated tolerance, screen coverage and frontier flags bit-exact, the
+priority queue equal up to near-ties."""
+import numpy as np
+import pytest
+
+from gpu_helpers import build_gpu, build_oracle
+from oracle import binding as ob
+
+pytestmark = pytest.mark.gpu
+
+W, H = 1920, 1080
+# Eigenvalues are in units of (node size)^2 and stored as float. The FP32
+# closed form is within EIG_RTOL x l1 of the FP64 Jacobi. The FP64 branch
+# (near-degenerate matrices, l3 < 1e-3 l1) is within float rounding of l1
+# (EIG64_RTOL x l1), and its smallest eigenvalue within L3_RTOL of itself --
+# the accuracy the branch exists for.
+EIG_RTOL = 2e-5
+EIG64_RTOL = 2.4e-7
+L3_RTOL = 1e-6
+SV_ATOL = 1e-4
+
+
+def oracle_frame(f):
+    o = ob.Frame()
+    o.width, o.height = f.width, f.height
+    for i in range(16):
+        o.transform[i] = f.transform[i]
+        o.transform_frozen[i] = f.transform_frozen[i]
+    for a in range(3):
+        o.box_min[a] = f.box_min[a]
+        o.box_max[a] = f.box_max[a]
+    o.lod_pixel_budget = f.lod_pixel_budget
+    o.point_size = f.point_size
+    o.drawlist_capacity = 131072
+    return o
+
+
+@pytest.fixture(scope="module")
+def analysed(c1_cloud):
+    from remobench_b200.lod import make_frame
+    cfg, cloud, bmin, bmax = c1_cloud
+    ctx, _ = build_gpu(cloud, bmin, bmax, cfg.batch_size)
+    tree = build_oracle(cloud, bmin, bmax, cfg.batch_size)
+    tree.accumulate(8)
+    f = make_frame(bmin, bmax, W, H, yaw=1.2, pitch=-0.5, radius_scale=0.5)
+    r = ctx.analyze(f, min_points=16, closure_margin=8, frontier_only=True, queue_capacity=4096)
+    return ctx, tree, f, r
+
+
+def test_rollup_exact(analysed):
+    ctx, tree, _, _ = analysed
+    g = ctx.rollup()
+    o, _ = tree.rolled_sums()
+    assert np.array_equal(g, o)
+    assert g[0, 0] == 8 * 262144  # the root holds every point
+
+
+def test_eigenvalues_within_tolerance(analysed):
+    ctx, tree, _, _ = analysed
+    a = ctx.analysis()
+    o = tree.analyze_fp64()
+    oe = np.array([list(x.eig) for x in o])
+    osv = np.array([x.surface_variation for x in o])
+    cnt = np.array([x.count for x in o])
+    m = cnt >= 3
+    assert np.array_equal(a["count"], cnt)
+    l1 = np.maximum(oe[:, 0], 1e-30)
+    err = np.abs(a["eig"].astype(np.float64) - oe) / l1[:, None]
+    fp64 = (a["flags"] & 1) != 0
+    assert np.all(err[m & ~fp64] <= EIG_RTOL), err[m & ~fp64].max()
+    if np.any(m & fp64):
+        assert np.all(err[m & fp64] <= EIG64_RTOL), err[m & fp64].max()
+        l3 = np.maximum(np.abs(oe[:, 2]), 1e-30)
+        e3 = np.abs(a["eig"][:, 2].astype(np.float64) - oe[:, 2]) / l3
+        assert np.all(e3[m & fp64] <= L3_RTOL), e3[m & fp64].max()
+    assert np.all(np.abs(a["surface_variation"][m] - osv[m]) <= SV_ATOL)
+
+
+def test_coverage_flags_closure_exact(analysed):
+    ctx, tree, f, _ = analysed
+    a = ctx.analysis()
+    p = ob.AnalysisParams()
+    p.min_points, p.closure_margin, p.current_batch, p.frontier_only, p.pixel_budget = 16, 8, 8, 1, 128.0
+    cov, flags, closed, score = tree.analysis_scores(oracle_frame(f), p, tree.analyze_fp64())
+    assert np.array_equal(a["coverage"], cov)
+    assert np.array_equal(a["flags"] & 6, flags)
+    assert np.array_equal(a["closed"], closed)
+    assert np.all(np.abs(a["score"] - score) <= SV_ATOL * np.maximum(cov, 1e-30) + 1e-7)
+
+
+def test_queue_is_the_top_k(analysed):
+    ctx, tree, f, r = analysed
+    q = ctx.queue()
+    a = ctx.analysis()
+    assert r.queue_length == len(q) > 0
+    assert r.overflow == 0
+    eligible = (a["score"] > 0) & ((a["flags"] & 4) != 0)
+    assert r.eligible == int(eligible.sum())
+    assert np.all(eligible[q])
+    # descending score, ties by node id
+    s = a["score"][q]
+    assert np.all(s[:-1] >= s[1:])
+    # the GPU queue is the top-K of the GPU scores
+    ids = np.nonzero(eligible)[0]
+    order = ids[np.lexsort((ids, -a["score"][ids]))]
+    assert np.array_equal(q, order[:len(q)])
+    # and, up to near-ties, the top-K of the FP64 oracle's scores
+    p = ob.AnalysisParams()
+    p.min_points, p.closure_margin, p.current_batch, p.frontier_only, p.pixel_budget = 16, 8, 8, 1, 128.0
+    _, flags, _, score = tree.analysis_scores(oracle_frame(f), p, tree.analyze_fp64())
+    oel = np.nonzero((score > 0) & ((flags & 4) != 0))[0]
+    otop = oel[np.argsort(-score[oel], kind="stable")][:len(q)]
+    overlap = len(set(q.tolist()) & set(otop.tolist())) / len(q)
+    assert overlap >= 0.98, overlap
+
+
+def test_refine_mask_marks_queue_prefix(analysed):
+    import torch
+    ctx, _, _, r = analysed
+    q = ctx.queue()
+    nn = len(ctx.nodes())
+    mask = torch.full((nn,), 9, dtype=torch.uint8, device="cuda")
+    budget = min(50, len(q))
+    ctx.refine(budget, mask)
+    m = mask.cpu().numpy()
+    assert set(np.nonzero(m)[0].tolist()) == set(q[:budget].tolist())
+    assert np.all(m[m != 0] == 1)

@@ -309,8 +309,14 @@ typedef struct rb_analysis_params {
     uint32_t frontier_only;    /* queue only nodes Refinement can open (1) */
     uint32_t queue_capacity;   /* top-K kept (<= 16384) */
     float pixel_budget;        /* the LOD cut's budget, to find the frontier (128) */
-    uint32_t pad;
+    uint32_t score_mode;       /* RB_SCORE_* */
 } rb_analysis_params;
+
+/* How Refinement ranks the frontier. PARTIAL: the current (partial) surface
+ * variation; CLOSED: closure-lagged -- only closed nodes score, the plain
+ * method; LEARNED: closed nodes by their surface variation, open nodes by
+ * their partial one plus the learned scorer's predicted correction. */
+enum { RB_SCORE_PARTIAL = 0, RB_SCORE_CLOSED = 1, RB_SCORE_LEARNED = 2 };
 
 typedef struct rb_analysis_result {
     uint32_t queue_length;
@@ -347,6 +353,29 @@ rb_status rb_read_rollup(struct rb_ctx* ctx, uint64_t* out16, uint32_t capacity,
  * last Analysis queue are written as 1 into the node mask at mask_dev (one
  * byte per node), which rb_render takes as force_large_dev. */
 rb_status rb_refine(struct rb_ctx* ctx, uint32_t budget, uint64_t mask_dev);
+
+/* The learned scorer (no reference counterpart: plans/04_NeuralPass.md is
+ * empty): a 16 -> 64 -> 64 -> 2 MLP, GELU, BF16 weights and activations, FP32
+ * accumulation, trained on the GPU with these entry points. Inputs are the 16
+ * per-node features rb_analyze logs (rb_read_features); outputs are the
+ * predicted change from the partial to the final surface variation (x 300)
+ * and a closure logit. Parameters are
+ * RB_MLP_NUM_PARAMS floats: W1[64][16], b1[64], W2[64][64], b2[64], W3[2][64], b3[2]. */
+#define RB_MLP_NUM_PARAMS 5378
+#define RB_NUM_FEATURES 16
+rb_status rb_read_features(struct rb_ctx* ctx, float* out16, uint32_t capacity, uint32_t* count);
+rb_status rb_mlp_init(struct rb_ctx* ctx, uint64_t seed);
+rb_status rb_mlp_set_params(struct rb_ctx* ctx, const float* params);   /* also restarts Adam */
+rb_status rb_mlp_get_params(struct rb_ctx* ctx, float* params);
+/* y_dev[2 n] = network(x_dev[16 n]); device pointers. */
+rb_status rb_mlp_predict(struct rb_ctx* ctx, uint64_t x_dev, uint32_t n, uint64_t y_dev);
+/* Gradient of the mean loss over n samples (targets t_dev[2 n]) into grad
+ * (host, RB_MLP_NUM_PARAMS floats), mean loss into *loss; no update. */
+rb_status rb_mlp_gradients(struct rb_ctx* ctx, uint64_t x_dev, uint64_t t_dev, uint32_t n, float* grad,
+                           float* loss);
+/* One Adam step on n samples; *loss (optional) receives the batch's mean loss. */
+rb_status rb_mlp_train_step(struct rb_ctx* ctx, uint64_t x_dev, uint64_t t_dev, uint32_t n, float lr,
+                            float* loss);
 
 /* Kernel timing (see rb_kernel_profile). */
 rb_status rb_set_profiling(struct rb_ctx* ctx, int on);

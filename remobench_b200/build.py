@@ -30,6 +30,7 @@ CUDA_UNITS = {
     "rb_capi.cu": [],
     "rb_noalloc.cu": [],
     "rb_analysis.cu": ["-fmad=false"],
+    "rb_mlp.cu": [],
 }
 
 

@@ -17,6 +17,8 @@ RB_ERR_INVALID_ARG, RB_ERR_CUDA, RB_ERR_OUT_OF_MEMORY, RB_ERR_STATE = 1, 2, 3, 4
 RB_ERR_RING, RB_ERR_CAPACITY, RB_ERR_NO_DEVICE, RB_ERR_UNSUPPORTED = 5, 6, 7, 8
 RB_PIPELINE_REMOLOD, RB_PIPELINE_SIMLOD, RB_PIPELINE_FLAT = 0, 1, 2
 RB_VOXEL_LOWEST_INDEX, RB_VOXEL_FIRST_COME = 0, 1
+RB_SCORE_PARTIAL, RB_SCORE_CLOSED, RB_SCORE_LEARNED = 0, 1, 2
+MLP_NUM_PARAMS, NUM_FEATURES = 5378, 16
 
 u32, u64, i32, f32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_float
 
@@ -85,7 +87,7 @@ class NodeInfo(ctypes.Structure):
 
 class AnalysisParams(ctypes.Structure):
     _fields_ = [("min_points", u32), ("closure_margin", u32), ("frontier_only", u32), ("queue_capacity", u32),
-                ("pixel_budget", f32), ("pad", u32)]
+                ("pixel_budget", f32), ("score_mode", u32)]
 
 
 class AnalysisResult(ctypes.Structure):
@@ -134,6 +136,13 @@ SIGNATURES = {
     "rb_read_queue": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_read_rollup": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_refine": (i32, [_vp, u32, u64]),
+    "rb_read_features": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
+    "rb_mlp_init": (i32, [_vp, u64]),
+    "rb_mlp_set_params": (i32, [_vp, _vp]),
+    "rb_mlp_get_params": (i32, [_vp, _vp]),
+    "rb_mlp_predict": (i32, [_vp, u64, u32, u64]),
+    "rb_mlp_gradients": (i32, [_vp, u64, u64, u32, _vp, ctypes.POINTER(f32)]),
+    "rb_mlp_train_step": (i32, [_vp, u64, u64, u32, f32, ctypes.POINTER(f32)]),
     "rb_set_profiling": (i32, [_vp, ctypes.c_int]),
     "rb_read_profile": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_reset_profile": (i32, [_vp]),

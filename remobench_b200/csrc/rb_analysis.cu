@@ -51,9 +51,14 @@ __global__ void __launch_bounds__(256) k_roll_level(Dev d, RollSum* roll, uint32
                 r.s2[2 * k] = a.s2lo[k];
                 r.s2[2 * k + 1] = a.s2hi[k];
             }
+            for (int k = 0; k < 3; k++) {
+                r.c1[k] = a.c1[k];
+                r.c2[k] = a.c2[k];
+            }
             r.lastTouched = a.count ? a.lastTouchedBatch : 0u;
             r.pad = 0;
         } else {
+            unsigned long long cc1[3] = {0, 0, 0}, cc2[3] = {0, 0, 0};
             u128 s1[3] = {0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0};
             u128 n = 0;
             uint32_t lt = 0;
@@ -74,6 +79,14 @@ __global__ void __launch_bounds__(256) k_roll_level(Dev d, RollSum* roll, uint32
                     s2[k] += c2 + o[pa[k]] * c1[pb[k]] + o[pb[k]] * c1[pa[k]] + cn * o[pa[k]] * o[pb[k]];
                 }
                 lt = cr.lastTouched > lt ? cr.lastTouched : lt;
+                for (int k = 0; k < 3; k++) {
+                    cc1[k] += cr.c1[k];
+                    cc2[k] += cr.c2[k];
+                }
+            }
+            for (int k = 0; k < 3; k++) {
+                r.c1[k] = cc1[k];
+                r.c2[k] = cc2[k];
             }
             r.n = (unsigned long long)n;
             for (int k = 0; k < 3; k++) r.s1[k] = (unsigned long long)s1[k];
@@ -183,7 +196,7 @@ __device__ __forceinline__ F4a mat(const float* m, float x, float y, float z) {
 
 // Per node: covariance, eigen-solve, metrics, screen coverage, score, queue key.
 __global__ void __launch_bounds__(256) k_analyze(Dev d, const RollSum* roll, NodeAnalysis* out,
-                                                 unsigned long long* keys, AnalysisParams prm, Frame f,
+                                                 float* features, AnalysisParams prm, Frame f,
                                                  AnalysisCounters* ac) {
     const uint32_t nn = d.ctr->numNodes;
     const float cube = fmaxf(fmaxf(f.boxMax[0] - f.boxMin[0], f.boxMax[1] - f.boxMin[1]), f.boxMax[2] - f.boxMin[2]);
@@ -287,11 +300,62 @@ __global__ void __launch_bounds__(256) k_analyze(Dev d, const RollSum* roll, Nod
         if (inner && !large && parentLarge) o.flags |= kAnalysisFrontier;
         o.coverage = cov2d;
         o.closed = (prm.currentBatch >= o.lastTouched + prm.closureMargin && r.n > 0) ? 1u : 0u;
-        float score = o.surfaceVariation * cov2d;
-        if (r.n < prm.minPoints) score = 0.0f;
-        o.score = score;
+        o.score = 0.0f;
         out[i] = o;
-        // queue key: score bits (non-negative float orders as unsigned), then low ids first
+        // the learned scorer's inputs (the training-data logger records these)
+        float* ft = features + (size_t)i * kNumFeatures;
+        const double nd = r.n ? (double)r.n : 1.0;
+        const double unit = ldexp(1.0, (int)(28u - lv));
+        ft[0] = log2f(1.0f + (float)r.n) * (1.0f / 24.0f);
+        ft[1] = (float)lv * (1.0f / 20.0f);
+        for (int k = 0; k < 3; k++) ft[2 + k] = r.n ? (float)((double)r.s1[k] / (nd * unit)) : 0.0f;
+        {
+            // normalised centred second moments (a uniform cube has 1/12 on the diagonal)
+            const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 2};
+            for (int k = 0; k < 6; k++) {
+                float v = 0.0f;
+                if (r.n >= 2) {
+                    const u128 s2 = ((u128)r.s2[2 * k + 1] << 64) | r.s2[2 * k];
+                    const i128 c = (i128)((u128)r.n * s2) - (i128)r.s1[pa[k]] * (i128)r.s1[pb[k]];
+                    v = (float)(i128ToDouble(c) / (nd * nd * unit * unit) * 12.0);
+                }
+                ft[5 + k] = v;
+            }
+        }
+        ft[11] = o.surfaceVariation * 3.0f;
+        ft[12] = o.planarity;
+        const bool leafNode = !inner;
+        const float fill = leafNode ? (float)d.numPoints[i] * (1.0f / 50000.0f) : (float)d.numVoxels[i] * (1.0f / 16384.0f);
+        ft[13] = fminf(fill, 4.0f);
+        float cvar = 0.0f;
+        if (r.n >= 2) {
+            for (int k = 0; k < 3; k++) {
+                const double m = (double)r.c1[k] / nd;
+                cvar += (float)(((double)r.c2[k] / nd - m * m) / (255.0 * 255.0));
+            }
+        }
+        ft[14] = cvar * (4.0f / 3.0f);
+        const float age = prm.currentBatch > o.lastTouched ? (float)(prm.currentBatch - o.lastTouched) : 0.0f;
+        ft[15] = fminf(age / (float)(prm.closureMargin ? prm.closureMargin : 1u), 2.0f);
+    }
+}
+
+// Score x coverage, the queue key, per node. In the learned mode an open
+// node's surface variation is its partial one plus the network's predicted
+// correction (output 0, x 1/300).
+__global__ void __launch_bounds__(256) k_score(Dev d, NodeAnalysis* out, const float* pred, unsigned long long* keys,
+                                               AnalysisParams prm, AnalysisCounters* ac) {
+    const uint32_t nn = d.ctr->numNodes;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
+        NodeAnalysis o = out[i];
+        float sv = o.surfaceVariation;
+        if (prm.scoreMode == kScoreClosed && !o.closed) sv = 0.0f;
+        // the network predicts the change from the partial surface variation to the final one
+        if (prm.scoreMode == kScoreLearned && !o.closed && pred)
+            sv = fminf(fmaxf(sv + pred[2 * i] * (1.0f / 300.0f), 0.0f), 1.0f / 3.0f);
+        float score = sv * o.coverage;
+        if (o.count < prm.minPoints) score = 0.0f;
+        out[i].score = score;
         const bool eligible = score > 0.0f && (prm.frontierOnly == 0u || (o.flags & kAnalysisFrontier));
         keys[i] = eligible ? (((unsigned long long)__float_as_uint(score) << 32) | (0xFFFFFFFFu - i)) : 0ull;
         if (eligible) atomicAdd(&ac->eligible, 1u);
@@ -405,9 +469,13 @@ __global__ void __launch_bounds__(256) k_refine_set(const uint32_t* queue, const
 void launchRollLevel(const Dev& d, RollSum* roll, uint32_t level, int grid, cudaStream_t s) {
     k_roll_level<<<grid, 256, 0, s>>>(d, roll, level);
 }
-void launchAnalyze(const Dev& d, const RollSum* roll, NodeAnalysis* out, unsigned long long* keys,
+void launchAnalyze(const Dev& d, const RollSum* roll, NodeAnalysis* out, float* features,
                    const AnalysisParams& p, const Frame& f, AnalysisCounters* ac, int grid, cudaStream_t s) {
-    k_analyze<<<grid, 256, 0, s>>>(d, roll, out, keys, p, f, ac);
+    k_analyze<<<grid, 256, 0, s>>>(d, roll, out, features, p, f, ac);
+}
+void launchScore(const Dev& d, NodeAnalysis* out, const float* predictions, unsigned long long* keys,
+                 const AnalysisParams& p, AnalysisCounters* ac, int grid, cudaStream_t s) {
+    k_score<<<grid, 256, 0, s>>>(d, out, predictions, keys, p, ac);
 }
 void launchQueue(const Dev& d, const unsigned long long* keys, uint32_t* hist, unsigned long long* cand,
                  uint32_t candCap, uint32_t K, uint32_t* queue, AnalysisCounters* ac, int grid, cudaStream_t s) {

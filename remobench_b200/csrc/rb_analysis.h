@@ -15,8 +15,19 @@ struct RollSum {
     unsigned long long n;
     unsigned long long s1[3];
     unsigned long long s2[12];
+    unsigned long long c1[3];  // Σ of the 8-bit r, g, b
+    unsigned long long c2[3];  // Σ of their squares
     uint32_t lastTouched;
     uint32_t pad;
+};
+
+constexpr int kNumFeatures = 16;
+
+// How Refinement ranks the frontier (rb_analysis_params.score_mode).
+enum ScoreMode : uint32_t {
+    kScorePartial = 0,     // current (partial) surface variation x coverage
+    kScoreClosed = 1,      // closure-lagged: closed nodes only, open nodes score 0
+    kScoreLearned = 2,     // closed: their surface variation; open: the MLP's prediction
 };
 
 enum AnalysisFlags : uint32_t {
@@ -45,7 +56,7 @@ struct AnalysisParams {
     uint32_t currentBatch;
     uint32_t frontierOnly;   // queue only nodes Refinement can open (kAnalysisFrontier)
     float pixelBudget;
-    uint32_t pad;
+    uint32_t scoreMode;      // ScoreMode
 };
 
 struct AnalysisCounters {
@@ -59,8 +70,11 @@ struct AnalysisCounters {
 };
 
 void launchRollLevel(const Dev& d, RollSum* roll, uint32_t level, int grid, cudaStream_t s);
-void launchAnalyze(const Dev& d, const RollSum* roll, NodeAnalysis* out, unsigned long long* keys,
+void launchAnalyze(const Dev& d, const RollSum* roll, NodeAnalysis* out, float* features,
                    const AnalysisParams& p, const Frame& f, AnalysisCounters* ac, int grid, cudaStream_t s);
+// Score and queue key per node; predictions (2 per node) are read in kScoreLearned mode.
+void launchScore(const Dev& d, NodeAnalysis* out, const float* predictions, unsigned long long* keys,
+                 const AnalysisParams& p, AnalysisCounters* ac, int grid, cudaStream_t s);
 void launchQueue(const Dev& d, const unsigned long long* keys, uint32_t* hist, unsigned long long* cand,
                  uint32_t candCap, uint32_t K, uint32_t* queue, AnalysisCounters* ac, int grid, cudaStream_t s);
 void launchRefineMask(const Dev& d, const uint32_t* queue, const AnalysisCounters* ac, uint32_t budget,

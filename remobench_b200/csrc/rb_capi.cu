@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -13,6 +14,7 @@
 #include "../../include/rb_capi.h"
 #include "rb_analysis.h"
 #include "rb_kernels.h"
+#include "rb_mlp.h"
 #include "rb_state.h"
 
 using rb::Counters;
@@ -24,14 +26,14 @@ enum KernelId : int {
     K_BUILD_BEGIN, K_BATCH_BEGIN, K_COUNT_FIRST, K_SPLIT, K_SPILL_COPY, K_RECOUNT, K_VOX_SAMPLE,
     K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END, K_ACCUMULATE, K_ACCUM_VERIFY,
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
-    K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_NUM
+    K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
     "k_vox_sample", "k_vox_commit", "k_alloc_chunks", "k_insert", "k_vox_store", "k_batch_end",
     "k_accumulate", "k_accum_verify", "k_sweep", "k_reset_root", "k_fb_clear", "k_node_flags",
     "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve", "k_roll_level", "k_analyze",
-    "k_queue", "k_refine"};
+    "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam"};
 
 struct Profiler {
     bool on = false;
@@ -111,6 +113,11 @@ struct rb_ctx {
     rb::AnalysisCounters* actr = nullptr;
     rb::AnalysisCounters* hostActr = nullptr;
     bool analyzed = false;
+    float* features = nullptr;
+    float* predictions = nullptr;
+    rb::MlpState mlp{};
+    bool mlpReady = false;
+    uint32_t adamT = 0;
     // host-ingest ring
     rb::Point* ingestRing = nullptr;
     uint32_t ingestSlots = 0;
@@ -325,6 +332,9 @@ void rb_release(rb_ctx* c) {
     if (c->hostActr) cudaFreeHost(c->hostActr);
     c->hostActr = nullptr;
     c->analyzed = false;
+    c->mlp = rb::MlpState{};
+    c->mlpReady = false;
+    c->adamT = 0;
     c->hostCtr = nullptr;
     c->hostSweep = nullptr;
     c->hostAccum = nullptr;
@@ -492,6 +502,14 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(c->acand, kQueueSortCap, "queue candidates");
     ALLOC(c->aqueue, kQueueSortCap, "queue");
     ALLOC(c->actr, 1, "analysis counters");
+    ALLOC(c->features, (uint64_t)N * rb::kIn, "scorer features");
+    ALLOC(c->predictions, (uint64_t)N * rb::kOut, "scorer predictions");
+    ALLOC(c->mlp.params, rb::kNumParams, "scorer parameters");
+    ALLOC(c->mlp.grad, rb::kNumParams, "scorer gradient");
+    ALLOC(c->mlp.m, rb::kNumParams, "Adam first moment");
+    ALLOC(c->mlp.v, rb::kNumParams, "Adam second moment");
+    ALLOC(c->mlp.wq, rb::kNumQuant, "scorer BF16 weights");
+    ALLOC(c->mlp.loss, 1, "scorer loss");
     c->ingestSlots = 3;
     ALLOC(c->ingestRing, (uint64_t)c->ingestSlots * cfg.slot_capacity, "ingest ring");
 #undef ALLOC
@@ -506,6 +524,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     RB_CUDA(c, cudaMallocHost(&c->hostRs, sizeof(rb::RenderScratch)));
     RB_CUDA(c, cudaMallocHost(&c->hostActr, sizeof(rb::AnalysisCounters)));
     RB_CUDA(c, rb::configureQueueSort(kQueueSortCap));
+    RB_CUDA(c, rb::configureMlp());
     for (uint32_t i = 0; i < c->ingestSlots; i++) {
         RB_CUDA(c, cudaEventCreateWithFlags(&c->slotFree[i], cudaEventDisableTiming));
         RB_CUDA(c, cudaEventCreateWithFlags(&c->slotFull[i], cudaEventDisableTiming));
@@ -953,14 +972,24 @@ rb_status rb_analyze(rb_ctx* c, const rb_frame* f, const rb_analysis_params* p, 
     ap.currentBatch = c->batchesConsumed;
     ap.frontierOnly = p->frontier_only;
     ap.pixelBudget = p->pixel_budget;
-    ap.pad = 0;
+    ap.scoreMode = p->score_mode;
+    if (p->score_mode > RB_SCORE_LEARNED) return fail(c, RB_ERR_INVALID_ARG, "unknown score_mode");
+    if (p->score_mode == RB_SCORE_LEARNED && !c->mlpReady)
+        return fail(c, RB_ERR_STATE, "learned scoring needs rb_mlp_init or rb_mlp_set_params first");
+    rb_status rst = readCounters(c);
+    if (rst != RB_OK) return rst;
+    const uint32_t numNodes = c->hostCtr->numNodes;
     const rb::Frame fr = toFrame(f);
     RB_CUDA(c, cudaEventRecord(c->evStart, s));
     RB_CUDA(c, cudaMemsetAsync(c->ahist, 0, 65536 * 4, s));
     RB_CUDA(c, cudaMemsetAsync(c->actr, 0, sizeof(rb::AnalysisCounters), s));
     for (int L = rb::kMaxDepth; L >= 0; L--)
         LAUNCH(c, K_ROLL, 0, rb::launchRollLevel(c->d, c->roll, (uint32_t)L, grid, s));
-    LAUNCH(c, K_ANALYZE, 0, rb::launchAnalyze(c->d, c->roll, c->analysis, c->akeys, ap, fr, c->actr, grid, s));
+    LAUNCH(c, K_ANALYZE, 0, rb::launchAnalyze(c->d, c->roll, c->analysis, c->features, ap, fr, c->actr, grid, s));
+    if (p->score_mode == RB_SCORE_LEARNED)
+        LAUNCH(c, K_MLP_PREDICT, numNodes,
+               rb::launchMlpPredict(c->mlp, c->features, numNodes, c->predictions, c->numSMs * 4, s));
+    LAUNCH(c, K_SCORE, 0, rb::launchScore(c->d, c->analysis, c->predictions, c->akeys, ap, c->actr, grid, s));
     LAUNCH(c, K_QUEUE, 0, rb::launchQueue(c->d, c->akeys, c->ahist, c->acand, kQueueSortCap, p->queue_capacity,
                                           c->aqueue, c->actr, grid, s));
     RB_CUDA(c, cudaGetLastError());
@@ -998,6 +1027,143 @@ rb_status rb_read_analysis(rb_ctx* c, rb_node_analysis* out, uint32_t capacity, 
     rb_status st = readCounters(c);
     if (st != RB_OK) return st;
     return copyOut(c, out, c->analysis, sizeof(rb_node_analysis), capacity, count, c->hostCtr->numNodes);
+}
+
+rb_status rb_read_features(rb_ctx* c, float* out, uint32_t capacity, uint32_t* count) {
+    if (!c || !count) return RB_ERR_INVALID_ARG;
+    if (!c->analyzed) return fail(c, RB_ERR_STATE, "read before rb_analyze");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    return copyOut(c, out, c->features, sizeof(float) * rb::kIn, capacity, count, c->hostCtr->numNodes);
+}
+
+static rb_status mlpUpload(rb_ctx* c, const float* params) {
+    RB_CUDA(c, cudaMemcpy(c->mlp.params, params, sizeof(float) * rb::kNumParams, cudaMemcpyHostToDevice));
+    RB_CUDA(c, cudaMemset(c->mlp.m, 0, sizeof(float) * rb::kNumParams));
+    RB_CUDA(c, cudaMemset(c->mlp.v, 0, sizeof(float) * rb::kNumParams));
+    rb::launchMlpQuantize(c->mlp, c->stream);
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->adamT = 0;
+    c->mlpReady = true;
+    return RB_OK;
+}
+
+static rb_status mlpCheck(rb_ctx* c) {
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT || !c->mlp.params)
+        return fail(c, RB_ERR_STATE, "the scorer lives in an allocated remolod/simlod context");
+    return RB_OK;
+}
+
+rb_status rb_mlp_init(rb_ctx* c, uint64_t seed) {
+    if (!c) return RB_ERR_INVALID_ARG;
+    rb_status st = mlpCheck(c);
+    if (st != RB_OK) return st;
+    RB_CUDA(c, cudaSetDevice(c->device));
+    // Glorot-uniform weights (Glorot & Bengio 2010), zero biases; splitmix64 stream
+    std::vector<float> p(rb::kNumParams, 0.0f);
+    uint64_t x = seed;
+    auto next = [&]() {
+        uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    auto fill = [&](int off, int rows, int cols) {
+        const double a = std::sqrt(6.0 / (double)(rows + cols));
+        for (int i = 0; i < rows * cols; i++) p[off + i] = (float)((2.0 * next() - 1.0) * a);
+    };
+    fill(rb::kPW1, rb::kHidden, rb::kIn);
+    fill(rb::kPW2, rb::kHidden, rb::kHidden);
+    fill(rb::kPW3, rb::kOut, rb::kHidden);
+    return mlpUpload(c, p.data());
+}
+
+rb_status rb_mlp_set_params(rb_ctx* c, const float* params) {
+    if (!c || !params) return RB_ERR_INVALID_ARG;
+    rb_status st = mlpCheck(c);
+    if (st != RB_OK) return st;
+    RB_CUDA(c, cudaSetDevice(c->device));
+    return mlpUpload(c, params);
+}
+
+rb_status rb_mlp_get_params(rb_ctx* c, float* params) {
+    if (!c || !params) return RB_ERR_INVALID_ARG;
+    rb_status st = mlpCheck(c);
+    if (st != RB_OK) return st;
+    if (!c->mlpReady) return fail(c, RB_ERR_STATE, "scorer not initialised");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    RB_CUDA(c, cudaMemcpy(params, c->mlp.params, sizeof(float) * rb::kNumParams, cudaMemcpyDeviceToHost));
+    return RB_OK;
+}
+
+rb_status rb_mlp_predict(rb_ctx* c, uint64_t x, uint32_t n, uint64_t y) {
+    if (!c || (n && (!x || !y))) return RB_ERR_INVALID_ARG;
+    rb_status st = mlpCheck(c);
+    if (st != RB_OK) return st;
+    if (!c->mlpReady) return fail(c, RB_ERR_STATE, "scorer not initialised");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    LAUNCH(c, K_MLP_PREDICT, n, rb::launchMlpPredict(c->mlp, reinterpret_cast<const float*>(x), n,
+                                                      reinterpret_cast<float*>(y), c->numSMs * 8, c->stream));
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return RB_OK;
+}
+
+static rb_status mlpGrad(rb_ctx* c, uint64_t x, uint64_t t, uint32_t n) {
+    RB_CUDA(c, cudaMemsetAsync(c->mlp.grad, 0, sizeof(float) * rb::kNumParams, c->stream));
+    RB_CUDA(c, cudaMemsetAsync(c->mlp.loss, 0, sizeof(float), c->stream));
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 63) / 64, (uint64_t)c->numSMs));
+    LAUNCH(c, K_MLP_GRAD, n, rb::launchMlpGrad(c->mlp, reinterpret_cast<const float*>(x),
+                                               reinterpret_cast<const float*>(t), n, grid, c->stream));
+    RB_CUDA(c, cudaGetLastError());
+    return RB_OK;
+}
+
+rb_status rb_mlp_gradients(rb_ctx* c, uint64_t x, uint64_t t, uint32_t n, float* grad, float* loss) {
+    if (!c || !x || !t || n == 0) return RB_ERR_INVALID_ARG;
+    rb_status st = mlpCheck(c);
+    if (st != RB_OK) return st;
+    if (!c->mlpReady) return fail(c, RB_ERR_STATE, "scorer not initialised");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    st = mlpGrad(c, x, t, n);
+    if (st != RB_OK) return st;
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (grad) RB_CUDA(c, cudaMemcpy(grad, c->mlp.grad, sizeof(float) * rb::kNumParams, cudaMemcpyDeviceToHost));
+    if (loss) {
+        RB_CUDA(c, cudaMemcpy(loss, c->mlp.loss, sizeof(float), cudaMemcpyDeviceToHost));
+        *loss /= (float)n;
+    }
+    return RB_OK;
+}
+
+rb_status rb_mlp_train_step(rb_ctx* c, uint64_t x, uint64_t t, uint32_t n, float lr, float* loss) {
+    if (!c || !x || !t || n == 0 || !(lr > 0.0f)) return RB_ERR_INVALID_ARG;
+    rb_status st = mlpCheck(c);
+    if (st != RB_OK) return st;
+    if (!c->mlpReady) return fail(c, RB_ERR_STATE, "scorer not initialised");
+    RB_CUDA(c, cudaSetDevice(c->device));
+    st = mlpGrad(c, x, t, n);
+    if (st != RB_OK) return st;
+    c->adamT += 1;
+    rb::AdamStep a;
+    a.lr = lr;
+    a.beta1 = 0.9f;
+    a.beta2 = 0.999f;
+    a.eps = 1e-8f;
+    a.bc1 = (float)(1.0 - std::pow(0.9, (double)c->adamT));
+    a.bc2 = (float)(1.0 - std::pow(0.999, (double)c->adamT));
+    LAUNCH(c, K_MLP_ADAM, 0, rb::launchMlpAdam(c->mlp, a, c->stream));
+    RB_CUDA(c, cudaGetLastError());
+    if (loss) {
+        RB_CUDA(c, cudaMemcpyAsync(loss, c->mlp.loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        RB_CUDA(c, cudaStreamSynchronize(c->stream));
+        *loss /= (float)n;
+    }
+    return RB_OK;
 }
 
 rb_status rb_read_queue(rb_ctx* c, uint32_t* ids, uint32_t capacity, uint32_t* count) {

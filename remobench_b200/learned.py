@@ -1,0 +1,217 @@
+"""The learned scorer's data, training and evaluation.
+
+- collect(): stream seeded configuration-1 clouds through the plain pipeline;
+  after every batch, rb_analyze logs the 16 features of every node (the
+  training-data logger); when the cloud is done, each logged open node is
+  paired with its final surface variation and whether it still gained points
+  (the (partial, final) pairs).
+- train(): Adam on those pairs with the CUDA forward/backward kernels
+  (rb_mlp_train_step); nothing is trained on the CPU.
+- evaluate(): at equal Refinement budgets, PSNR of the refined LOD render
+  against the flat render of the same points, for the three ways of ranking the
+  frontier: closure-lagged (the plain method: open nodes wait for closure),
+  partial (current surface variation, no learning) and learned (open nodes by
+  the network's prediction of their final surface variation).
+"""
+import math
+
+import numpy as np
+
+from . import capi, synth
+from .camera import orbit_path
+from .lod import Context, DeviceRing, make_frame
+
+MIN_POINTS = 16
+
+
+def _cloud(seed, num_points, batch):
+    cfg = synth.config(1, seed=seed, num_points=num_points, batch_size=batch)
+    pts = synth.generate(cfg)
+    bmin, bmax = synth.scene_box(cfg)
+    return cfg, pts, bmin, bmax
+
+
+SPLIT_LIMIT = 5000  # leaf split limit of the scorer experiments (deeper trees, larger frontiers)
+SV_SCALE = 300.0    # the network's output 0 is the surface-variation correction x SV_SCALE
+
+
+def collect(seeds, num_points=8 * 262144, batch=262144, closure_margin=2):
+    """(X, T, info): features of open nodes after each batch, with targets
+    (final surface variation x 3, 1 if the node gains no further points)."""
+    xs, ts = [], []
+    for seed in seeds:
+        cfg, pts, bmin, bmax = _cloud(seed, num_points, batch)
+        ctx = Context(slot_capacity=batch, time_budget_ms=0.0, max_batches_per_build=1,
+                      max_points_per_node=SPLIT_LIMIT)
+        ctx.allocate(len(pts), bmin, bmax)
+        ring = DeviceRing(pts, batch, slots=ctx.cfg.ring_slots, slot_capacity=batch)
+        frame = make_frame(bmin, bmax, 640, 360)
+        snaps = []
+        consumed = 0
+        while consumed < ring.num_batches:
+            ring.upload_window(consumed)
+            consumed = ctx.build(ring.ring, ring.sizes, ring.uploaded, ring.num_batches).batches_consumed
+            ctx.analyze(frame, min_points=MIN_POINTS, closure_margin=closure_margin)
+            a = ctx.analysis()
+            snaps.append((ctx.features(), a["count"].copy(), a["closed"].copy()))
+        final = ctx.analysis()
+        for feat, cnt, closed in snaps:
+            nn = len(cnt)
+            sel = (cnt >= MIN_POINTS) & (closed == 0)
+            idx = np.nonzero(sel)[0]
+            xs.append(feat[idx])
+            # residual target: (final - partial) surface variation x SV_SCALE (feature 11 is partial x 3)
+            t0 = (final["surface_variation"][:nn][idx] - feat[idx, 11] / 3.0) * SV_SCALE
+            t1 = (final["count"][:nn][idx] == cnt[idx]).astype(np.float32)
+            ts.append(np.stack([t0, t1], 1).astype(np.float32))
+        ctx.close()
+    X = np.concatenate(xs).astype(np.float32)
+    T = np.concatenate(ts).astype(np.float32)
+    return X, T
+
+
+def train(ctx, X, T, epochs=40, batch=2048, lr=3e-3, seed=0):
+    """Adam on the GPU; returns the per-epoch mean training loss."""
+    import torch
+    rng = np.random.default_rng(seed)
+    xd = torch.from_numpy(X).cuda()
+    td = torch.from_numpy(T).cuda()
+    n = len(X)
+    batch = max(1, min(batch, n))
+    history = []
+    for ep in range(epochs):
+        perm = torch.from_numpy(rng.permutation(n)).cuda()
+        xs, tsh = xd[perm].contiguous(), td[perm].contiguous()
+        step_lr = lr * 0.5 * (1.0 + math.cos(math.pi * ep / epochs))
+        for k in range(0, n - batch + 1, batch):
+            ctx.mlp_train_step(xs[k:k + batch], tsh[k:k + batch], step_lr)
+        _, loss = ctx.mlp_gradients(xd, td)
+        history.append(loss)
+    return history
+
+
+def predict(ctx, X):
+    import torch
+    xd = torch.from_numpy(np.ascontiguousarray(X, dtype=np.float32)).cuda()
+    y = torch.empty((len(X), 2), dtype=torch.float32, device="cuda")
+    ctx.mlp_predict(xd, y)
+    return y.cpu().numpy()
+
+
+def psnr(a_rgba, b_rgba):
+    a = a_rgba.view(np.uint8).reshape(-1, 4)[:, :3].astype(np.float64)
+    b = b_rgba.view(np.uint8).reshape(-1, 4)[:, :3].astype(np.float64)
+    mse = np.mean((a - b) ** 2)
+    return float("inf") if mse == 0 else 10.0 * math.log10(255.0 ** 2 / mse)
+
+
+def evaluate(params, seed, num_points=8 * 262144, batch=262144, stop_batch=None, closure_margin=2,
+             fractions=(0.05, 0.10, 0.20, 0.40), views=3, width=960, height=540, budget_px=64.0):
+    """PSNR versus flat for each ranking and budget, averaged over `views`
+    orbit frames, on the tree after `stop_batch` batches of a held-out cloud."""
+    import torch
+    cfg, pts, bmin, bmax = _cloud(seed, num_points, batch)
+    nb = (len(pts) + batch - 1) // batch
+    stop = nb // 2 if stop_batch is None else stop_batch
+    ctx = Context(slot_capacity=batch, time_budget_ms=0.0, max_batches_per_build=1,
+                  max_points_per_node=SPLIT_LIMIT)
+    ctx.allocate(len(pts), bmin, bmax)
+    ring = DeviceRing(pts, batch, slots=ctx.cfg.ring_slots, slot_capacity=batch)
+    consumed = 0
+    while consumed < stop:
+        ring.upload_window(consumed)
+        consumed = ctx.build(ring.ring, ring.sizes, min(ring.uploaded, stop), ring.num_batches).batches_consumed
+    if params is not None:
+        ctx.mlp_set_params(params)
+    flat_ctx = Context(pipeline=capi.RB_PIPELINE_FLAT)
+    flat_ctx.allocate(len(pts), bmin, bmax)
+    ingested = torch.from_numpy(pts[:consumed * batch].view(np.float32).reshape(-1, 4)).cuda()
+    nn = len(ctx.nodes())
+    mask = torch.zeros(nn, dtype=torch.uint8, device="cuda")
+    fb = torch.empty(width * height, dtype=torch.int64, device="cuda")
+    rgba = torch.empty(width * height, dtype=torch.int32, device="cuda")
+    modes = {"closure_lagged": capi.RB_SCORE_CLOSED, "partial": capi.RB_SCORE_PARTIAL}
+    if params is not None:
+        modes["learned"] = capi.RB_SCORE_LEARNED
+    out = {m: {f: [] for f in fractions} for m in modes}
+    out["none"] = []
+    path = orbit_path(bmin, bmax, views, seed=seed + 1000)
+    for (yaw, pitch, rs) in path:
+        frame = make_frame(bmin, bmax, width, height, yaw=yaw, pitch=pitch, radius_scale=rs, budget=budget_px)
+        flat_ctx.render_flat(frame, ingested, fb, rgba)
+        truth = rgba.cpu().numpy().copy()
+        ctx.render(frame, fb, rgba)
+        out["none"].append(psnr(rgba.cpu().numpy(), truth))
+        # the frontier Refinement can open, from the partial ranking's eligibility
+        ctx.analyze(frame, min_points=MIN_POINTS, closure_margin=closure_margin, score_mode=capi.RB_SCORE_PARTIAL,
+                    queue_capacity=16384)
+        a = ctx.analysis()
+        frontier = int(np.sum(((a["flags"] & 4) != 0) & (a["count"] >= MIN_POINTS)))
+        for name, mode in modes.items():
+            ctx.analyze(frame, min_points=MIN_POINTS, closure_margin=closure_margin, score_mode=mode,
+                        queue_capacity=16384)
+            for f in fractions:
+                k = int(round(f * frontier))
+                ctx.refine(k, mask)
+                ctx.render(frame, fb, rgba, force_large=mask)
+                out[name][f].append(psnr(rgba.cpu().numpy(), truth))
+    result = {"seed": seed, "stop_batch": stop, "points": consumed * batch, "nodes": nn, "frontier": frontier,
+              "psnr_none": float(np.mean(out["none"]))}
+    for name in modes:
+        result[name] = {f"{int(f * 100)}%": float(np.mean(out[name][f])) for f in fractions}
+    ctx.close()
+    flat_ctx.close()
+    return result
+
+
+def main(argv=None):
+    """Collect, train, evaluate; prints one JSON line.
+
+    python -m remobench_b200.learned [--train-seeds 16] [--eval-seeds 4] [--points 524288]
+    """
+    import argparse
+    import json
+    import time
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train-seeds", type=int, default=16)
+    ap.add_argument("--eval-seeds", type=int, default=4)
+    ap.add_argument("--points", type=int, default=8 * 262144)
+    ap.add_argument("--batch", type=int, default=262144)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--margin", type=int, default=2)
+    ap.add_argument("--save", default=None, help="write the trained parameters (.npy)")
+    args = ap.parse_args(argv)
+    t0 = time.time()
+    train_seeds = list(range(100, 100 + args.train_seeds))
+    eval_seeds = list(range(900, 900 + args.eval_seeds))
+    X, T = collect(train_seeds, args.points, args.batch, args.margin)
+    Xv, Tv = collect(eval_seeds, args.points, args.batch, args.margin)
+    t_collect = time.time() - t0
+    cfg, _, bmin, bmax = _cloud(1, args.batch, args.batch)
+    ctx = Context(slot_capacity=args.batch)
+    ctx.allocate(args.batch, bmin, bmax)
+    ctx.mlp_init(1)
+    hist = train(ctx, X, T, epochs=args.epochs)
+    params = ctx.mlp_params()
+    if args.save:
+        np.save(args.save, params)
+    pv = predict(ctx, Xv)
+    # errors of the final surface variation: partial + correction, against partial alone
+    sv_err_learned = float(np.mean(np.abs(pv[:, 0] - Tv[:, 0]) / SV_SCALE))
+    sv_err_partial = float(np.mean(np.abs(Tv[:, 0]) / SV_SCALE))
+    closure_acc = float(np.mean((pv[:, 1] > 0) == (Tv[:, 1] > 0.5)))
+    evals = [evaluate(params, s, args.points, args.batch, closure_margin=args.margin) for s in eval_seeds]
+    frontier = float(np.mean([e["frontier"] for e in evals]))
+    summary = {}
+    for mode in ("closure_lagged", "partial", "learned"):
+        summary[mode] = {k: float(np.mean([e[mode][k] for e in evals])) for k in evals[0][mode]}
+    print(json.dumps({"train_pairs": int(len(X)), "heldout_pairs": int(len(Xv)), "final_train_loss": hist[-1],
+                      "heldout_sv_mae_learned": sv_err_learned, "heldout_sv_mae_partial": sv_err_partial,
+                      "heldout_closure_accuracy": closure_acc, "psnr_no_refinement": float(np.mean([e["psnr_none"] for e in evals])),
+                      "psnr": summary, "frontier_nodes": frontier, "collect_s": round(t_collect, 1),
+                      "total_s": round(time.time() - t0, 1)}))
+
+
+if __name__ == "__main__":
+    main()

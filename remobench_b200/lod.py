@@ -174,13 +174,14 @@ class Context:
         return g
 
     def analyze(self, frame, min_points=16, closure_margin=8, frontier_only=True, queue_capacity=4096,
-                pixel_budget=None):
+                pixel_budget=None, score_mode=0):
         p = capi.AnalysisParams()
         p.min_points = int(min_points)
         p.closure_margin = int(closure_margin)
         p.frontier_only = 1 if frontier_only else 0
         p.queue_capacity = int(queue_capacity)
         p.pixel_budget = float(frame.lod_pixel_budget if pixel_budget is None else pixel_budget)
+        p.score_mode = int(score_mode)
         r = capi.AnalysisResult()
         self._ok(capi.lib().rb_analyze(self.h, ctypes.byref(frame), ctypes.byref(p), ctypes.byref(r)))
         return r
@@ -206,6 +207,42 @@ class Context:
         out = np.zeros((n.value, 16), dtype=np.uint64)
         self._ok(capi.lib().rb_read_rollup(self.h, ctypes.c_void_p(out.ctypes.data), n.value, ctypes.byref(n)))
         return out
+
+    def features(self):
+        n = ctypes.c_uint32()
+        self._ok(capi.lib().rb_read_features(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, capi.NUM_FEATURES), dtype=np.float32)
+        self._ok(capi.lib().rb_read_features(self.h, ctypes.c_void_p(out.ctypes.data), n.value, ctypes.byref(n)))
+        return out
+
+    def mlp_init(self, seed):
+        self._ok(capi.lib().rb_mlp_init(self.h, int(seed)))
+
+    def mlp_set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == capi.MLP_NUM_PARAMS
+        self._ok(capi.lib().rb_mlp_set_params(self.h, ctypes.c_void_p(p.ctypes.data)))
+
+    def mlp_params(self):
+        p = np.zeros(capi.MLP_NUM_PARAMS, dtype=np.float32)
+        self._ok(capi.lib().rb_mlp_get_params(self.h, ctypes.c_void_p(p.ctypes.data)))
+        return p
+
+    def mlp_predict(self, x_dev, y_dev):
+        self._ok(capi.lib().rb_mlp_predict(self.h, x_dev.data_ptr(), int(x_dev.shape[0]), y_dev.data_ptr()))
+
+    def mlp_gradients(self, x_dev, t_dev):
+        g = np.zeros(capi.MLP_NUM_PARAMS, dtype=np.float32)
+        loss = ctypes.c_float()
+        self._ok(capi.lib().rb_mlp_gradients(self.h, x_dev.data_ptr(), t_dev.data_ptr(), int(x_dev.shape[0]),
+                                             ctypes.c_void_p(g.ctypes.data), ctypes.byref(loss)))
+        return g, loss.value
+
+    def mlp_train_step(self, x_dev, t_dev, lr, want_loss=False):
+        loss = ctypes.c_float()
+        self._ok(capi.lib().rb_mlp_train_step(self.h, x_dev.data_ptr(), t_dev.data_ptr(), int(x_dev.shape[0]),
+                                              float(lr), ctypes.byref(loss) if want_loss else None))
+        return loss.value if want_loss else None
 
     def refine(self, budget, mask):
         self._ok(capi.lib().rb_refine(self.h, int(budget), mask.data_ptr()))

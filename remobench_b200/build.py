@@ -98,16 +98,18 @@ def build_host(force=False):
     hdrs = _headers(HOST) + [os.path.join(ROOT, "include", "rb_capi.h")]
     lib_srcs = [s for s in srcs if not s.endswith("harness_main.cpp")]
     out = os.path.join(LIB, "librb_host.so")
+    cuda = os.path.dirname(os.path.dirname(_nvcc()))
     common = ["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-I", os.path.join(ROOT, "include"),
-              "-I", CSRC, "-I", HOST]
+              "-I", CSRC, "-I", HOST, "-I", os.path.join(cuda, "include")]
     rpath = "-Wl,-rpath,$ORIGIN"
+    # the CUDA runtime is linked statically, as nvcc links librb_cuda.so
+    cudart = ["-L", os.path.join(cuda, "lib64"), "-lcudart_static", "-ldl", "-lrt", "-lpthread"]
     if force or _stale(out, lib_srcs + hdrs):
-        _run(common + ["-shared", "-o", out] + lib_srcs + ["-L", LIB, "-lrb_cuda", "-lrb_synth", rpath,
-                                                           "-lpthread"])
+        _run(common + ["-shared", "-o", out] + lib_srcs + ["-L", LIB, "-lrb_cuda", "-lrb_synth", rpath] + cudart)
     main = os.path.join(HOST, "harness_main.cpp")
     exe = os.path.join(LIB, "rb_harness")
     if os.path.exists(main) and (force or _stale(exe, [main, out] + hdrs)):
-        _run(common + ["-o", exe, main, "-L", LIB, "-lrb_host", "-lrb_cuda", "-lrb_synth", rpath, "-lpthread"])
+        _run(common + ["-o", exe, main, "-L", LIB, "-lrb_host", "-lrb_cuda", "-lrb_synth", rpath] + cudart)
     return out
 
 

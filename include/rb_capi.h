@@ -77,14 +77,14 @@ typedef struct rb_config {
     uint32_t ring_slots;             /* 50 */
     uint32_t slot_capacity;          /* 1000000 points per ring slot */
     uint32_t max_batches_per_build;  /* 20 */
-    float time_budget_ms;            /* 10; 0 = no wall-clock budget */
+    float time_budget_ms;            /* 10; 0 = none. Device time since the rb_build call began, checked before each batch */
     uint32_t voxel_mode;             /* RB_VOXEL_* */
     uint32_t accumulate;             /* fold Accumulate into every build (remolod) */
     uint32_t spilled_capacity;       /* 10,000,000 */
     uint32_t spilling_nodes_capacity;/* 100,000 */
     uint32_t drawlist_capacity;      /* 131072 */
     uint64_t safety_margin;          /* 200,000,000 bytes */
-    uint32_t use_graphs;             /* capture each batch's kernels in a CUDA graph */
+    uint32_t use_graphs;             /* 1: each batch is one CUDA graph launch, expand loop on the device; 0: host-driven loop */
     uint32_t reserved[7];
 } rb_config;
 

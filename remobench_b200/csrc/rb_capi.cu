@@ -26,14 +26,16 @@ enum KernelId : int {
     K_BUILD_BEGIN, K_BATCH_BEGIN, K_COUNT_FIRST, K_SPLIT, K_SPILL_COPY, K_RECOUNT, K_VOX_SAMPLE,
     K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END, K_ACCUMULATE, K_ACCUM_VERIFY,
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
-    K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM, K_NUM
+    K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
+    K_HASH_RESET, K_EXPAND_COND, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
     "k_vox_sample", "k_vox_commit", "k_alloc_chunks", "k_insert", "k_vox_store", "k_batch_end",
     "k_accumulate", "k_accum_verify", "k_sweep", "k_reset_root", "k_fb_clear", "k_node_flags",
     "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve", "k_roll_level", "k_analyze",
-    "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam"};
+    "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam", "k_hash_reset",
+    "k_expand_cond"};
 
 struct Profiler {
     bool on = false;
@@ -118,6 +120,10 @@ struct rb_ctx {
     rb::MlpState mlp{};
     bool mlpReady = false;
     uint32_t adamT = 0;
+    // device-driven batches: one graph per batch, the ring descriptor it reads
+    cudaGraphExec_t batchGraph = nullptr;
+    bool graphTried = false;
+    rb::RingDesc* hostRing = nullptr;  // pinned staging for d.ring
     // host-ingest ring
     rb::Point* ingestRing = nullptr;
     uint32_t ingestSlots = 0;
@@ -199,6 +205,10 @@ rb_status readCounters(rb_ctx* c) {
 __global__ void k_build_begin(Counters* c) {
     c->buildStamp += 1;
     c->numDirty = 0;
+    c->callBatches = 0;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    c->buildStartNs = t;
 }
 
 // One batch through addBatch's phases (remolod_octree.cu:940-1060). Returns
@@ -207,11 +217,7 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
     const Dev& d = c->d;
     cudaStream_t s = c->stream;
     *stopped = false;
-    if (c->hostCtr->overflowFlags & rb::kOvfBacklog) {
-        // an overflowed batch left table entries its list could not name
-        RB_CUDA(c, cudaMemsetAsync(d.hashKeys, 0xFF, ((size_t)d.hashMask + 1) * 8, s));
-        RB_CUDA(c, cudaMemsetAsync(d.hashVals, 0xFF, ((size_t)d.hashMask + 1) * 8, s));
-    }
+    LAUNCH(c, K_HASH_RESET, 0, rb::launchHashReset(d, c->numSMs * 8, s));
     LAUNCH(c, K_BATCH_BEGIN, 1, rb::launchBatchBegin(d, s));
     LAUNCH(c, K_COUNT_FIRST, n, rb::launchCountFirst(d, pts, n, pointGrid(c, n), s));
     const int fixedGrid = c->numSMs * 4;
@@ -237,6 +243,37 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
     LAUNCH(c, K_VOX_STORE, 0, rb::launchVoxStore(d, fixedGrid, s));
     LAUNCH(c, K_BATCH_END, 1, rb::launchBatchEnd(d, n, s));
     RB_CUDA(c, cudaGetLastError());
+    return RB_OK;
+}
+
+// The device-driven path: on unless profiling (per-kernel events need
+// separate launches) or use_graphs is 0; captured at the first build.
+bool graphPath(rb_ctx* c) {
+    if (!c->cfg.use_graphs || c->prof.on) return false;
+    if (!c->graphTried) {
+        c->graphTried = true;
+        const int pointGrid = c->numSMs * 8, fixedGrid = c->numSMs * 4;
+        if (rb::captureBatchGraph(c->d, pointGrid, fixedGrid, &c->batchGraph) != cudaSuccess) c->batchGraph = nullptr;
+    }
+    return c->batchGraph != nullptr;
+}
+
+// Launches of one graph batch, for the per-kernel counts: ten fixed kernels
+// per batch, four per pass of the expand loop.
+void countGraphLaunches(rb_ctx* c, uint64_t batches, uint64_t itersBefore, uint64_t done, uint64_t points) {
+    // each built batch adds 1 + (its split passes) to expandIters
+    const uint64_t iters = c->hostCtr->expandIters;
+    const uint64_t passes = iters >= itersBefore + done ? iters - itersBefore - done : 0u;
+    for (int k : {K_HASH_RESET, K_BATCH_BEGIN, K_COUNT_FIRST, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT,
+                  K_VOX_STORE, K_BATCH_END})
+        c->prof.launches[k] += batches;
+    c->prof.launches[K_EXPAND_COND] += batches + passes;
+    for (int k : {K_SPLIT, K_SPILL_COPY, K_RECOUNT}) c->prof.launches[k] += passes;
+    for (int k : {K_COUNT_FIRST, K_VOX_SAMPLE, K_INSERT}) c->prof.units[k] += points;
+}
+
+rb_status uploadRing(rb_ctx* c) {
+    RB_CUDA(c, cudaMemcpyAsync(c->d.ring, c->hostRing, sizeof(rb::RingDesc), cudaMemcpyHostToDevice, c->stream));
     return RB_OK;
 }
 
@@ -294,7 +331,7 @@ void rb_config_defaults(rb_config* cfg) {
     cfg->spilling_nodes_capacity = 100000;
     cfg->drawlist_capacity = 131072;
     cfg->safety_margin = 200000000ull;
-    cfg->use_graphs = 0;
+    cfg->use_graphs = 1;
 }
 
 rb_status rb_create(const rb_config* cfg, rb_ctx** out) {
@@ -331,6 +368,11 @@ void rb_release(rb_ctx* c) {
     if (c->hostRs) cudaFreeHost(c->hostRs);
     if (c->hostActr) cudaFreeHost(c->hostActr);
     c->hostActr = nullptr;
+    if (c->batchGraph) cudaGraphExecDestroy(c->batchGraph);
+    c->batchGraph = nullptr;
+    c->graphTried = false;
+    if (c->hostRing) cudaFreeHost(c->hostRing);
+    c->hostRing = nullptr;
     c->analyzed = false;
     c->mlp = rb::MlpState{};
     c->mlpReady = false;
@@ -483,12 +525,14 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.spillLeaf, d.spillCap, "spilled point leaves");
     ALLOC(d.spillNodes, nextPow2(d.spillingCap), "spilling nodes");
     ALLOC(d.splitRecs, d.spillingCap, "split records");
-    ALLOC(d.hashKeys, hashSize, "voxel cell table keys");
-    ALLOC(d.hashVals, hashSize, "voxel cell table values");
+    ALLOC(d.hashSlots, hashSize, "voxel cell table");
     ALLOC(d.hashNew, d.newCap, "new voxel cells");
     ALLOC(d.hashNewNode, d.newCap, "new voxel nodes");
     ALLOC(d.hashNewSlot, d.newCap, "new voxel slots");
+    ALLOC(d.hashNewCell, d.newCap, "new voxel cell indices");
+    ALLOC(d.hashNewColor, d.newCap, "new voxel colours");
     ALLOC(d.ctr, 1, "counters");
+    ALLOC(d.ring, 1, "ring descriptor");
     ALLOC(d.sweep, 1, "sweep stats");
     ALLOC(d.accumGlobals, 1, "accumulator globals");
     ALLOC(c->vis, N, "visible flags");
@@ -513,8 +557,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     c->ingestSlots = 3;
     ALLOC(c->ingestRing, (uint64_t)c->ingestSlots * cfg.slot_capacity, "ingest ring");
 #undef ALLOC
-    RB_CUDA(c, cudaMemsetAsync(d.hashKeys, 0xFF, (size_t)hashSize * 8, c->stream));
-    RB_CUDA(c, cudaMemsetAsync(d.hashVals, 0xFF, (size_t)hashSize * 8, c->stream));
+    RB_CUDA(c, cudaMemsetAsync(d.hashSlots, 0xFF, (size_t)hashSize * 16, c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.ctr, 0, sizeof(Counters), c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.accumGlobals, 0, sizeof(rb::AccumGlobals), c->stream));
     RB_CUDA(c, cudaMallocHost(&c->hostCtr, sizeof(Counters)));
@@ -523,6 +566,9 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     RB_CUDA(c, cudaMallocHost(&c->hostAccum, sizeof(rb::AccumGlobals)));
     RB_CUDA(c, cudaMallocHost(&c->hostRs, sizeof(rb::RenderScratch)));
     RB_CUDA(c, cudaMallocHost(&c->hostActr, sizeof(rb::AnalysisCounters)));
+    RB_CUDA(c, cudaMallocHost(&c->hostRing, sizeof(rb::RingDesc)));
+    std::memset(c->hostRing, 0, sizeof(rb::RingDesc));
+    RB_CUDA(c, cudaMemsetAsync(d.ring, 0, sizeof(rb::RingDesc), c->stream));
     RB_CUDA(c, rb::configureQueueSort(kQueueSortCap));
     RB_CUDA(c, rb::configureMlp());
     for (uint32_t i = 0; i < c->ingestSlots; i++) {
@@ -545,7 +591,7 @@ rb_status rb_reset(rb_ctx* c) {
     RB_CUDA(c, cudaStreamSynchronize(c->stream));
     c->batchesConsumed = 0;
     c->accumAll = true;
-    return RB_OK;
+    return readCounters(c);  // the host mirror starts from the reset counters
 }
 
 static rb_status buildFrom(rb_ctx* c, const rb::Point* ring, const uint32_t* sizes, uint32_t slots,
@@ -553,15 +599,44 @@ static rb_status buildFrom(rb_ctx* c, const rb::Point* ring, const uint32_t* siz
     const auto t0 = std::chrono::steady_clock::now();
     const uint32_t first = c->batchesConsumed;
     const uint32_t avail = numUploaded > first ? numUploaded - first : 0u;
-    const uint32_t nb = std::min(avail, maxBatches);
+    uint32_t nb = std::min(avail, maxBatches);
+    for (uint32_t i = 0; i < std::min(slots, numUploaded); i++)
+        if (sizes[i] > slotCap) return fail(c, RB_ERR_CAPACITY, "batch larger than its ring slot");
+    const bool graphs = graphPath(c);
+    if (graphs) {
+        if (slots > rb::kMaxRingSlots) return fail(c, RB_ERR_CAPACITY, "more ring slots than a device build handles");
+        rb::RingDesc& r = *c->hostRing;
+        r.base = reinterpret_cast<unsigned long long>(ring);
+        r.slotCap = slotCap;
+        r.numSlots = slots;
+        r.numUploaded = numUploaded;
+        r.streamMode = 0;
+        r.first = 0;
+        r.batchSize = 0;
+        r.total = 0;
+        r.budgetNs = c->cfg.time_budget_ms > 0.0f ? (unsigned long long)(c->cfg.time_budget_ms * 1e6) : 0ull;
+        for (uint32_t i = 0; i < slots; i++) r.sizes[i] = sizes[i];
+        rb_status st = uploadRing(c);
+        if (st != RB_OK) return st;
+    }
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
     LAUNCH(c, K_BUILD_BEGIN, 1, (k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr)));
     uint32_t done = 0;
     bool stopped = false;
+    if (graphs) {
+        const uint64_t itersBefore = c->hostCtr->expandIters;
+        const uint64_t pointsBefore = c->hostCtr->numPointsProcessed;
+        for (uint32_t k = 0; k < nb; k++) RB_CUDA(c, cudaGraphLaunch(c->batchGraph, c->stream));
+        rb_status st = readCounters(c);
+        if (st != RB_OK) return st;
+        done = c->hostCtr->batchletIndex - first;
+        stopped = c->hostCtr->batchStop && c->hostCtr->stopReason == rb::kStopMemory;
+        countGraphLaunches(c, nb, itersBefore, done, c->hostCtr->numPointsProcessed - pointsBefore);
+        nb = 0;  // the batches ran on the device
+    }
     for (uint32_t b = first; b < first + nb; b++) {
         const uint32_t slot = b % slots;
         const uint32_t n = sizes[slot];
-        if (n > slotCap) return fail(c, RB_ERR_CAPACITY, "batch larger than its ring slot");
         rb_status st = runBatch(c, ring + (uint64_t)slot * slotCap, n, b, &stopped);
         if (st != RB_OK) return st;
         if (stopped) break;
@@ -625,6 +700,26 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
     RB_CUDA(c, cudaSetDevice(c->device));
     const uint64_t nb = (n + batchSize - 1) / batchSize;
     const uint32_t S = c->ingestSlots;
+    const uint32_t firstBatch = c->batchesConsumed;
+    if ((uint64_t)firstBatch + nb > 0xFFFFFFFFull) return fail(c, RB_ERR_CAPACITY, "too many batches");
+    const bool graphs = graphPath(c);
+    uint64_t itersBefore = 0, pointsBefore = 0;
+    if (graphs) {
+        rb::RingDesc& r = *c->hostRing;
+        r.base = reinterpret_cast<unsigned long long>(c->ingestRing);
+        r.slotCap = c->cfg.slot_capacity;
+        r.numSlots = S;
+        r.numUploaded = firstBatch + (uint32_t)nb;
+        r.streamMode = 1;
+        r.first = firstBatch;
+        r.batchSize = batchSize;
+        r.total = n;
+        r.budgetNs = 0;
+        rb_status st = uploadRing(c);
+        if (st != RB_OK) return st;
+        itersBefore = c->hostCtr->expandIters;
+        pointsBefore = c->hostCtr->numPointsProcessed;
+    }
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
     LAUNCH(c, K_BUILD_BEGIN, 1, (k_build_begin<<<1, 1, 0, c->stream>>>(c->d.ctr)));
     // the copy stream fills slot (b % S) once the compute stream released it
@@ -651,9 +746,16 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
         const uint64_t first = b * batchSize;
         const uint32_t cnt = (uint32_t)std::min<uint64_t>(batchSize, n - first);
         RB_CUDA(c, cudaStreamWaitEvent(c->stream, c->slotFull[slot], 0));
-        rb_status st = runBatch(c, c->ingestRing + (uint64_t)slot * c->cfg.slot_capacity, cnt,
-                                c->batchesConsumed, &stopped);
-        if (st != RB_OK) return st;
+        rb_status st = RB_OK;
+        if (graphs) {
+            // the graph finds batch first + b at slot b % S itself; a batch the
+            // memory check stops leaves the rest of the run as no-ops
+            RB_CUDA(c, cudaGraphLaunch(c->batchGraph, c->stream));
+        } else {
+            st = runBatch(c, c->ingestRing + (uint64_t)slot * c->cfg.slot_capacity, cnt, c->batchesConsumed,
+                          &stopped);
+            if (st != RB_OK) return st;
+        }
         RB_CUDA(c, cudaEventRecord(c->slotFree[slot], c->stream));
         if (stopped) break;
         c->batchesConsumed++;
@@ -680,6 +782,14 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
     RB_CUDA(c, cudaEventRecord(c->evStop, c->stream));
     RB_CUDA(c, cudaEventSynchronize(c->evStop));
     RB_CUDA(c, cudaStreamSynchronize(c->copyStream));
+    if (graphs) {
+        rb_status st = readCounters(c);
+        if (st != RB_OK) return st;
+        c->batchesConsumed = c->hostCtr->batchletIndex;
+        done = c->batchesConsumed - firstBatch;
+        stopped = c->hostCtr->batchStop && c->hostCtr->stopReason == rb::kStopMemory;
+        countGraphLaunches(c, nb, itersBefore, done, c->hostCtr->numPointsProcessed - pointsBefore);
+    }
     if (out) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, c->evStart, c->evStop);

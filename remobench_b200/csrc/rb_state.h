@@ -13,6 +13,8 @@
 
 #include <stdint.h>
 
+#include <vector_types.h>
+
 namespace rb {
 
 constexpr int kMaxDepth = 20;                 // remolod_structures.cuh:18
@@ -67,7 +69,37 @@ struct Counters {
     // dirty list for Accumulate
     uint32_t numDirty;
     uint32_t buildStamp;
-    uint32_t pad2;
+    // device-driven batches: the batch being built, read by every phase kernel
+    // launched without explicit points (pts == nullptr)
+    uint32_t curN;
+    unsigned long long curPts;    // device address of the batch's first point
+    unsigned long long buildStartNs;  // %globaltimer at the start of the build call
+    uint32_t lastStamp;           // splitIter stamp of the last split
+    uint32_t stopReason;          // 0 none, kStopMemory, kStopNoBatch, kStopTime
+    uint32_t expandGuard;         // expand passes of this batch (loop bound)
+    uint32_t hashNeedsClear;      // the cell table holds entries its list cannot name
+    uint32_t callBatches;         // batches built since the build call began
+    uint32_t pad3;
+};
+
+enum StopReason : uint32_t { kStopMemory = 1u, kStopNoBatch = 2u, kStopTime = 3u };
+
+// Where batch b lives, for device-driven builds (PointSource's BatchView,
+// include/remo/PointSource.h:43-67). Ring mode: slot b % numSlots holds
+// sizes[slot] points. Stream mode (host ingest): batch b is the (b - first)-th
+// of a run of total points cut into batchSize-point batches.
+constexpr uint32_t kMaxRingSlots = 256;
+struct RingDesc {
+    unsigned long long base;      // device address of slot 0
+    uint32_t slotCap;             // points per slot
+    uint32_t numSlots;
+    uint32_t numUploaded;         // batches [0, numUploaded) are readable
+    uint32_t streamMode;          // 0 ring, 1 stream
+    uint32_t first;               // stream mode: batch index of the run's first batch
+    uint32_t batchSize;           // stream mode
+    unsigned long long total;     // stream mode: points in the run
+    unsigned long long budgetNs;  // device time budget of the call, 0 = none
+    uint32_t sizes[kMaxRingSlots];
 };
 
 enum OverflowBits : uint32_t {
@@ -157,13 +189,17 @@ struct Dev {
     uint32_t* spillLeaf;
     uint32_t* spillNodes;    // [spillingCap] nodes whose counter crossed the limit
     SplitRec* splitRecs;     // [spillingCap]
-    unsigned long long* hashKeys;  // [hashMask + 1]
-    unsigned long long* hashVals;
+    // the batch's new-cell table: one 16-byte slot per cell, key (node << 21 |
+    // cell) and value (global point index << 32 | colour) in the same sector
+    ulonglong2* hashSlots;   // [hashMask + 1], kHashEmpty in both halves: free
     uint32_t* hashNew;       // [newCap] slots inserted this batch
     uint32_t* hashNewNode;   // node of each new cell
     uint32_t* hashNewSlot;   // slot of the new voxel within its node
+    uint32_t* hashNewCell;   // cell index (x + 128 y + 16384 z) of each new cell
+    uint32_t* hashNewColor;  // colour of its representative point
     uint32_t* dirtyList;     // [maxNodes]
     Counters* ctr;
+    RingDesc* ring;
     SweepStats* sweep;
     AccumGlobals* accumGlobals;
     // capacities and constants

@@ -12,6 +12,8 @@
 // operations in the same order.
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "rb_kernels.h"
 #include "rb_state.h"
 
@@ -70,23 +72,93 @@ __device__ __forceinline__ void countAt(const Dev& d, uint32_t leaf) {
     }
 }
 
-__global__ void k_batch_begin(Dev d) {
+__device__ __forceinline__ unsigned long long globalTimerNs() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Batch start (kernel_construct's loop head, remolod_octree.cu:1190-1240): the
+// memory check, and for device-driven builds the batch cursor -- which slot
+// holds batch batchletIndex and how many points it has -- and the call's time
+// budget. A stopped batch leaves every later phase kernel a no-op.
+__global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     Counters* c = d.ctr;
-    const bool stop = c->refOffset + d.safetyMargin >= d.persistentCapacity;
-    c->batchStop = stop ? 1u : 0u;
-    c->memCapacityReached = stop ? 1u : 0u;
+    uint32_t reason = 0;
+    if (fromRing) {
+        const RingDesc* r = d.ring;
+        const uint32_t b = c->batchletIndex;
+        if (b >= r->numUploaded) {
+            reason = kStopNoBatch;
+        } else {
+            uint32_t slot, n;
+            if (r->streamMode) {
+                const uint32_t rel = b - r->first;
+                const unsigned long long off = (unsigned long long)rel * r->batchSize;
+                slot = rel % r->numSlots;
+                n = off < r->total ? (uint32_t)min((unsigned long long)r->batchSize, r->total - off) : 0u;
+            } else {
+                slot = b % r->numSlots;
+                n = r->sizes[slot < kMaxRingSlots ? slot : 0u];
+            }
+            if (n > r->slotCap) n = r->slotCap;
+            c->curPts = r->base + (unsigned long long)slot * r->slotCap * sizeof(Point);
+            c->curN = n;
+        }
+    }
+    if (reason == 0 && c->refOffset + d.safetyMargin >= d.persistentCapacity) reason = kStopMemory;
+    // the budget is checked between batches: a call always builds its first batch
+    if (reason == 0 && fromRing && d.ring->budgetNs != 0ull && c->callBatches > 0u &&
+        globalTimerNs() - c->buildStartNs > d.ring->budgetNs)
+        reason = kStopTime;
+    if (reason == kStopMemory) c->memCapacityReached = 1u;
+    else if (reason == 0) c->memCapacityReached = 0u;
+    c->batchStop = reason ? 1u : 0u;
+    c->stopReason = reason;
     c->numSpill = 0;
     c->numSpilled = 0;
     c->numNew = 0;
     c->numSplit = 0;
     c->spillChunkTotal = 0;
     c->iter = 1;
+    c->expandGuard = 0;
+    c->hashNeedsClear = 0;  // k_hash_reset ran before this kernel
+}
+
+// Empties the whole cell table after a batch overflowed it (its list of new
+// cells could not name every entry, so k_vox_store could not clear them).
+__global__ void __launch_bounds__(256) k_hash_reset(Dev d) {
+    if (d.ctr->hashNeedsClear == 0u) return;
+    const uint32_t size = d.hashMask + 1u;
+    const ulonglong2 empty = make_ulonglong2(kHashEmpty, kHashEmpty);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x)
+        d.hashSlots[i] = empty;
+}
+
+// The expand loop's condition for device-driven builds: another split pass
+// while the last count found spilling nodes. expandGuard bounds the loop even
+// if the counts never settle (max_expand_iters <= 31 passes are needed).
+__global__ void k_expand_cond(Dev d, cudaGraphConditionalHandle h) {
+    Counters* c = d.ctr;
+    const uint32_t g = ++c->expandGuard;
+    const bool more = c->batchStop == 0u && c->numSpill > 0u && g <= 40u;
+    cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 // Iteration 1 of expand (doCounting over the batch, remolod_octree.cu:225-229):
 // descend every batch point, remember its leaf, count it there.
+// pts == nullptr: the batch at the device cursor (Counters::curPts / curN).
+#define RB_BATCH_AT_CURSOR(d, pts, n)                                   \
+    do {                                                                \
+        if ((pts) == nullptr) {                                         \
+            (pts) = reinterpret_cast<const Point*>((d).ctr->curPts);    \
+            (n) = (d).ctr->curN;                                        \
+        }                                                               \
+    } while (0)
+
 __global__ void __launch_bounds__(256) k_count_first(Dev d, const Point* __restrict__ pts, uint32_t n) {
     if (d.ctr->batchStop) return;
+    RB_BATCH_AT_CURSOR(d, pts, n);
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const uint32_t i = base + threadIdx.x;
@@ -118,9 +190,16 @@ __device__ __forceinline__ uint32_t stepIfSplit(const Dev& d, uint32_t cur, cons
     return (uint32_t)d.child[cur * 8u + ci];
 }
 
+// prevStamp == 0: device-driven; the stamp of the split just made, and no
+// recount once the pass limit is reached (the host loop does not launch it).
 __global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict__ pts, uint32_t n,
                                                  uint32_t prevStamp) {
     if (d.ctr->batchStop) return;
+    if (prevStamp == 0u) {
+        if (d.ctr->iter > d.maxExpandIters) return;
+        prevStamp = d.ctr->lastStamp;
+    }
+    RB_BATCH_AT_CURSOR(d, pts, n);
     const uint32_t ns = d.ctr->numSpilled < d.spillCap ? d.ctr->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -208,6 +287,9 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
     __shared__ uint32_t s_runPts, s_runChunks;
     Counters* c = d.ctr;
     if (c->batchStop) return;
+    // stamp 0: device-driven, (batch << 5) | pass as the host loop would pass it;
+    // read before any thread reaches the barriers below, after which c->iter moves
+    if (stamp == 0u) stamp = (c->batchletIndex << 5) | c->iter;
     uint32_t ns = c->numSpill;
     if (ns > d.spillingCap) ns = d.spillingCap;
     if (ns == 0) {
@@ -330,6 +412,7 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
         c->numSpilled = total;
         c->nodesSplit += acc;
         c->numSpill = 0;
+        c->lastStamp = stamp;
         c->iter += 1;
     }
 }
@@ -388,24 +471,31 @@ __device__ __forceinline__ uint32_t hashSlot(unsigned long long key, uint32_t ma
 __device__ void hashInsert(const Dev& d, unsigned long long key, unsigned long long val) {
     uint32_t slot = hashSlot(key, d.hashMask);
     for (uint32_t probe = 0; probe < 256u; probe++) {
-        unsigned long long cur = d.hashKeys[slot];
+        unsigned long long* ks = &d.hashSlots[slot].x;
+        unsigned long long* vs = &d.hashSlots[slot].y;
+        unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(ks);
         if (cur == kHashEmpty) {
-            cur = atomicCAS(&d.hashKeys[slot], kHashEmpty, key);
+            cur = atomicCAS(ks, kHashEmpty, key);
             if (cur == kHashEmpty) {
                 const uint32_t e = atomicAdd(&d.ctr->numNew, 1u);
-                if (e < d.newCap) d.hashNew[e] = slot;
-                else atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
+                if (e < d.newCap) {
+                    d.hashNew[e] = slot;
+                } else {
+                    atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
+                    d.ctr->hashNeedsClear = 1u;
+                }
                 cur = key;
             }
         }
         if (cur == key) {
-            if (d.voxelMode == 0u) atomicMin(&d.hashVals[slot], val);
-            else atomicCAS(&d.hashVals[slot], kHashEmpty, val);
+            if (d.voxelMode == 0u) atomicMin(vs, val);
+            else atomicCAS(vs, kHashEmpty, val);
             return;
         }
         slot = (slot + 1u) & d.hashMask;
     }
     atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
+    d.ctr->hashNeedsClear = 1u;
 }
 
 // voxelSampling (remolod_octree.cu:677-740) + sampleVoxel's test (:95-119):
@@ -416,6 +506,7 @@ __device__ void hashInsert(const Dev& d, unsigned long long key, unsigned long l
 __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restrict__ pts, uint32_t n) {
     const Counters* c = d.ctr;
     if (c->batchStop) return;
+    RB_BATCH_AT_CURSOR(d, pts, n);
     const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
@@ -435,12 +526,15 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
         }
         uint32_t x20 = 0, y20 = 0, z20 = 0, x28 = 0, y28 = 0, z28 = 0;
         if (active) {
-            x20 = quant20(p.x, d.boxMin[0], d.octreeSize);
-            y20 = quant20(p.y, d.boxMin[1], d.octreeSize);
-            z20 = quant20(p.z, d.boxMin[2], d.octreeSize);
             x28 = quant28(p.x, d.boxMin[0], d.octreeSize);
             y28 = quant28(p.y, d.boxMin[1], d.octreeSize);
             z28 = quant28(p.z, d.boxMin[2], d.octreeSize);
+            // 2^28 d / size is 2^8 times 2^20 d / size exactly (power-of-two
+            // scaling commutes with round-to-nearest), so the 20-bit coordinate
+            // is the 28-bit one shifted; only a saturated conversion differs
+            x20 = x28 < 0xFFFFFF00u ? x28 >> 8 : quant20(p.x, d.boxMin[0], d.octreeSize);
+            y20 = y28 < 0xFFFFFF00u ? y28 >> 8 : quant20(p.y, d.boxMin[1], d.octreeSize);
+            z20 = z28 < 0xFFFFFF00u ? z28 >> 8 : quant20(p.z, d.boxMin[2], d.octreeSize);
         }
         uint32_t cur = 0;
         for (uint32_t level = 0; level < (uint32_t)kMaxDepth; level++) {
@@ -461,6 +555,8 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
                 if (nx < 0) active = false;
                 else cur = (uint32_t)nx;
             }
+            // most levels of a warp hold no new cell: skip the match there
+            if (!__any_sync(0xFFFFFFFFu, key != kHashEmpty)) continue;
             const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
             if (key != kHashEmpty) {
                 int leader;
@@ -488,12 +584,16 @@ __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
         const uint32_t e = base + threadIdx.x;
         uint32_t node = kNone;
         if (e < nnew) {
+            // the table is final here: move the cell out of it and free the slot
             const uint32_t slot = d.hashNew[e];
-            const unsigned long long key = d.hashKeys[slot];
-            node = (uint32_t)(key >> 21);
-            const uint32_t vi = (uint32_t)(key & 0x1FFFFFull);
+            const ulonglong2 kv = d.hashSlots[slot];
+            d.hashSlots[slot] = make_ulonglong2(kHashEmpty, kHashEmpty);
+            node = (uint32_t)(kv.x >> 21);
+            const uint32_t vi = (uint32_t)(kv.x & 0x1FFFFFull);
             atomicOr(gridWordsAt(d, d.grid[node]) + (vi >> 5), 1u << (vi & 31u));
             d.hashNewNode[e] = node;
+            d.hashNewCell[e] = vi;
+            d.hashNewColor[e] = (uint32_t)(kv.y & 0xFFFFFFFFull);
         }
         // one counter bump per warp and node
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, node);
@@ -609,6 +709,7 @@ __global__ void __launch_bounds__(256) k_alloc_chunks(Dev d) {
 __global__ void __launch_bounds__(256) k_insert(Dev d, const Point* __restrict__ pts, uint32_t n) {
     Counters* c = d.ctr;
     if (c->batchStop) return;
+    RB_BATCH_AT_CURSOR(d, pts, n);
     const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
@@ -649,22 +750,17 @@ __global__ void __launch_bounds__(256) k_insert(Dev d, const Point* __restrict__
 }
 
 // insertVoxels (remolod_octree.cu:918-938): every new cell's voxel at its cell
-// centre (:124-134) with its representative's colour; then the table entry is
-// cleared for the next batch.
+// centre (:124-134) with its representative's colour, from the compact lists
+// k_vox_commit made.
 __global__ void __launch_bounds__(256) k_vox_store(Dev d) {
     const Counters* c = d.ctr;
     if (c->batchStop) return;
     const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
     const uint32_t ppc = d.ppc;
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nnew; e += gridDim.x * blockDim.x) {
-        const uint32_t hs = d.hashNew[e];
-        const unsigned long long key = d.hashKeys[hs];
-        const unsigned long long val = d.hashVals[hs];
-        d.hashKeys[hs] = kHashEmpty;
-        d.hashVals[hs] = kHashEmpty;
         const uint32_t node = d.hashNewNode[e];
         const uint32_t s = d.hashNewSlot[e];
-        const uint32_t vi = (uint32_t)(key & 0x1FFFFFull);
+        const uint32_t vi = d.hashNewCell[e];
         const uint32_t px = vi & 127u, py = (vi >> 7) & 127u, pz = vi >> 14;
         const uint32_t lv = d.level[node];
         const float nodeSize = __fdiv_rn(d.octreeSize, __int_as_float((int)((127u + lv) << 23)));
@@ -675,7 +771,7 @@ __global__ void __launch_bounds__(256) k_vox_store(Dev d) {
         v.x = __fadd_rn(mnx, __fdiv_rn(__fmul_rn(nodeSize, __fadd_rn((float)px, 0.5f)), 128.0f));
         v.y = __fadd_rn(mny, __fdiv_rn(__fmul_rn(nodeSize, __fadd_rn((float)py, 0.5f)), 128.0f));
         v.z = __fadd_rn(mnz, __fdiv_rn(__fmul_rn(nodeSize, __fadd_rn((float)pz, 0.5f)), 128.0f));
-        v.color = (uint32_t)(val & 0xFFFFFFFFull);
+        v.color = d.hashNewColor[e];
         if (s < d.numVoxelChunks[node] * ppc) {
             const uint32_t phys = d.tablePool[d.vxTableOff[node] + s / ppc];
             if (phys != kNone) chunkPoints(d, phys)[s % ppc] = v;
@@ -683,9 +779,12 @@ __global__ void __launch_bounds__(256) k_vox_store(Dev d) {
     }
 }
 
+// n == kNone: the batch at the device cursor.
 __global__ void k_batch_end(Dev d, uint32_t n) {
     Counters* c = d.ctr;
     if (c->batchStop) return;
+    if (n == kNone) n = c->curN;
+    c->callBatches += 1;
     if (c->numAllocatedChunks > c->chunkPoolSize) c->chunkPoolSize = c->numAllocatedChunks;
     c->batchletIndex += 1;
     c->numPointsProcessed += n;
@@ -725,6 +824,7 @@ __global__ void k_reset_root(Dev d) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         Counters z = {};
         z.buildStamp = c->buildStamp;
+        z.hashNeedsClear = c->hashNeedsClear;  // stale table entries outlive a reset
         *c = z;
         c->refOffset = 16;
         c->numNodes = 1;
@@ -759,7 +859,8 @@ __global__ void k_reset_root(Dev d) {
 
 // ------------------------------------------------------------------ launches
 
-void launchBatchBegin(const Dev& d, cudaStream_t s) { k_batch_begin<<<1, 1, 0, s>>>(d); }
+void launchBatchBegin(const Dev& d, cudaStream_t s) { k_batch_begin<<<1, 1, 0, s>>>(d, 0u); }
+void launchHashReset(const Dev& d, int grid, cudaStream_t s) { k_hash_reset<<<grid, 256, 0, s>>>(d); }
 void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_count_first<<<grid, 256, 0, s>>>(d, pts, n);
 }
@@ -781,5 +882,80 @@ void launchVoxStore(const Dev& d, int grid, cudaStream_t s) { k_vox_store<<<grid
 void launchBatchEnd(const Dev& d, uint32_t n, cudaStream_t s) { k_batch_end<<<1, 1, 0, s>>>(d, n); }
 void launchSweep(const Dev& d, int grid, cudaStream_t s) { k_sweep<<<grid, 256, 0, s>>>(d); }
 void launchResetRoot(const Dev& d, int grid, cudaStream_t s) { k_reset_root<<<grid, 256, 0, s>>>(d); }
+
+// One batch as a CUDA graph: the phase kernels of runBatch with the expand
+// loop as a conditional WHILE node, every kernel reading its batch from the
+// device cursor. One graph launch builds the batch at batchletIndex with no
+// host round trip; a stopped batch (memory, no batch uploaded, time budget)
+// runs through as no-ops.
+cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGraphExec_t* out) {
+    *out = nullptr;
+    cudaStream_t cs = nullptr, bs = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        if (cs) cudaStreamDestroy(cs);
+        return e;
+    }
+    bool capturing = false;
+    do {
+        if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) break;
+        capturing = true;
+        k_hash_reset<<<pointGrid, 256, 0, cs>>>(d);
+        k_batch_begin<<<1, 1, 0, cs>>>(d, 1u);
+        k_count_first<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        cudaStreamCaptureStatus status;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &ndeps)) != cudaSuccess) break;
+        cudaGraphConditionalHandle h;
+        if ((e = cudaGraphConditionalHandleCreate(&h, g, 0u, 0u)) != cudaSuccess) break;
+        k_expand_cond<<<1, 1, 0, cs>>>(d, h);
+        if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &ndeps)) != cudaSuccess) break;
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cond;
+        if ((e = cudaGraphAddNode(&cond, g, deps, ndeps, &cp)) != cudaSuccess) break;
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        if ((e = cudaStreamUpdateCaptureDependencies(cs, &cond, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+            break;
+        // the loop body: split, make room, recount, decide
+        if ((e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+            cudaSuccess)
+            break;
+        k_split<<<1, 1024, 0, bs>>>(d, 0u);
+        k_spill_copy<<<fixedGrid, 256, 0, bs>>>(d);
+        k_recount<<<pointGrid, 256, 0, bs>>>(d, nullptr, 0u, 0u);
+        k_expand_cond<<<1, 1, 0, bs>>>(d, h);
+        cudaGraph_t bodyOut = nullptr;
+        if ((e = cudaStreamEndCapture(bs, &bodyOut)) != cudaSuccess) break;
+        k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        k_vox_commit<<<fixedGrid, 256, 0, cs>>>(d);
+        k_alloc_chunks<<<fixedGrid, 256, 0, cs>>>(d);
+        k_insert<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        k_vox_store<<<fixedGrid, 256, 0, cs>>>(d);
+        k_batch_end<<<1, 1, 0, cs>>>(d, kNone);
+        capturing = false;
+        if ((e = cudaStreamEndCapture(cs, &graph)) != cudaSuccess) break;
+        e = cudaGraphInstantiate(out, graph, 0ull);
+    } while (false);
+    if (capturing) {
+        cudaGraph_t dropped = nullptr;
+        cudaStreamEndCapture(cs, &dropped);
+        if (dropped) cudaGraphDestroy(dropped);
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(bs);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+    }
+    return e;
+}
 
 }  // namespace rb

@@ -8,7 +8,8 @@ from oracle import binding as ob
 def build_gpu(cloud, bmin, bmax, batch_size, budget=0, per_call=20, **cfg):
     from remobench_b200.lod import Context, DeviceRing
     slot_cap = cfg.pop("slot_capacity", batch_size)
-    ctx = Context(slot_capacity=slot_cap, time_budget_ms=0.0, max_batches_per_build=per_call, **cfg)
+    cfg.setdefault("time_budget_ms", 0.0)
+    ctx = Context(slot_capacity=slot_cap, max_batches_per_build=per_call, **cfg)
     ctx.allocate(len(cloud), bmin, bmax, budget)
     ring = DeviceRing(cloud, batch_size, slots=ctx.cfg.ring_slots, slot_capacity=slot_cap)
     consumed, calls = 0, 0

@@ -82,3 +82,34 @@ def test_first_come_voxels_are_members_of_their_cell(c1_cloud, c1_pair):
     for i in np.nonzero(nodes["num_voxels"])[0][:50]:
         for v in ctx.node_voxels(int(i)):
             assert int(v["color"]) in colours
+
+
+def test_host_loop_and_device_graph_agree(c1_cloud, c1_pair):
+    """The host-driven expand loop (use_graphs=0, one sync per pass) and the
+    device-driven batch graph (default) build the same tree and counters."""
+    cfg, cloud, bmin, bmax = c1_cloud
+    ctx, tree = c1_pair
+    host, _ = build_gpu(cloud, bmin, bmax, cfg.batch_size, use_graphs=0)
+    compare_nodes(host, tree)
+    compare_accums(host, tree)
+    a, b = host.stats(), ctx.stats()
+    for f in ("num_points", "num_voxels", "num_nodes", "expand_iters", "nodes_split", "spilled_points",
+              "persistent_offset", "num_allocated_chunks", "chunk_pool_size", "batchlet_index"):
+        assert getattr(a, f) == getattr(b, f), f
+    # both paths count the same kernels per batch; the graph adds its loop test
+    pa = {k: v["launches"] for k, v in host.profile().items()}
+    pb = {k: v["launches"] for k, v in ctx.profile().items()}
+    for k in ("k_count_first", "k_split", "k_spill_copy", "k_vox_sample", "k_insert", "k_batch_end"):
+        assert pa[k] == pb[k], (k, pa[k], pb[k])
+    assert pb["k_expand_cond"] == pb["k_count_first"] + pb["k_split"]
+
+
+def test_device_time_budget_paces_but_keeps_the_tree(c1_cloud, c1_pair):
+    """A 1 us device budget stops each call after its first batch; the calls
+    together still build the oracle's tree."""
+    cfg, cloud, bmin, bmax = c1_cloud
+    ctx, tree = c1_pair
+    paced, calls = build_gpu(cloud, bmin, bmax, cfg.batch_size, time_budget_ms=0.001)
+    assert calls == 8
+    assert np.array_equal(paced.nodes(), ctx.nodes())
+    compare_accums(paced, tree)

@@ -174,6 +174,11 @@ struct Dev {
     uint32_t* vxTableOff;
     uint32_t* vxTableCap;
     uint32_t* splitIter;     // 1-based expand iteration of the split in this batch, 0: none
+    // ancestors of every node, root first: row n holds (id, grid) of the nodes
+    // at levels 0 .. level(n)-1 above n. Written once when n is created (its
+    // ancestors are inner then and keep their grids), so one row gives every
+    // grid a point of n must test, with no pointer chase.
+    uint2* anc;              // [maxNodes * kMaxDepth]
     uint32_t* dirtyStamp;
     AccumI* accum;
     // storage: one arena in 16-byte units holding grids (256 KB), point chunks

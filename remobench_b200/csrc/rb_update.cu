@@ -333,6 +333,15 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
             const uint32_t base = nn + 8u * k;
             const uint32_t lv = d.level[node] + 1u;
             const uint32_t X = d.nodeX[node], Y = d.nodeY[node], Z = d.nodeZ[node];
+            uint32_t g = d.grid[node];
+            if (g == kNone) {
+                g = arenaAlloc(d, kGridUnits);
+                d.grid[node] = g;
+                atomicAdd(&c->numGrids, 1u);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
+                          (unsigned long long)refAllocSize(kGridBytes));
+            }
+            const uint2* prow = d.anc + (size_t)node * kMaxDepth;
             for (uint32_t i = 0; i < 8; i++) {
                 const uint32_t ch = base + i;
 #pragma unroll
@@ -356,6 +365,9 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
                 d.dirtyStamp[ch] = 0;
                 AccumI z = {};
                 d.accum[ch] = z;
+                uint2* crow = d.anc + (size_t)ch * kMaxDepth;
+                for (uint32_t l = 0; l + 1u < lv; l++) crow[l] = prow[l];
+                crow[lv - 1u] = make_uint2(node, g);
                 d.child[node * 8u + i] = (int32_t)ch;
             }
             d.splitIter[node] = stamp;
@@ -377,14 +389,6 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
             d.numPointChunks[node] = 0;
             d.ptTableOff[node] = kNone;
             d.ptTableCap[node] = 0;
-            uint32_t g = d.grid[node];
-            if (g == kNone) {
-                g = arenaAlloc(d, kGridUnits);
-                d.grid[node] = g;
-                atomicAdd(&c->numGrids, 1u);
-                atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
-                          (unsigned long long)refAllocSize(kGridBytes));
-            }
             r.grid = g;
             d.splitRecs[k] = r;
             if (d.dirtyStamp[node] != c->buildStamp) {
@@ -467,23 +471,30 @@ __device__ __forceinline__ uint32_t hashSlot(unsigned long long key, uint32_t ma
     return (uint32_t)h & mask;
 }
 
-// Inserts (key -> min val) into the per-batch cell table.
-__device__ void hashInsert(const Dev& d, unsigned long long key, unsigned long long val) {
-    uint32_t slot = hashSlot(key, d.hashMask);
+// Records a claimed table slot in the batch's list of new cells.
+__device__ __forceinline__ void listNewCell(const Dev& d, uint32_t e, uint32_t slot) {
+    if (e < d.newCap) {
+        d.hashNew[e] = slot;
+    } else {
+        atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
+        d.ctr->hashNeedsClear = 1u;
+    }
+}
+
+// Inserts (key -> min val) into the per-batch cell table, probing from slot.
+__device__ void hashInsertFrom(const Dev& d, unsigned long long key, unsigned long long val, uint32_t slot) {
     for (uint32_t probe = 0; probe < 256u; probe++) {
         unsigned long long* ks = &d.hashSlots[slot].x;
         unsigned long long* vs = &d.hashSlots[slot].y;
-        unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(ks);
+        // key and value in one 16-byte read: a present key whose value is
+        // already lower needs no atomic (values only decrease)
+        const ulonglong2 kv = __ldcg(&d.hashSlots[slot]);
+        unsigned long long cur = kv.x;
+        if (cur == key && kv.y <= val && d.voxelMode == 0u) return;
         if (cur == kHashEmpty) {
             cur = atomicCAS(ks, kHashEmpty, key);
             if (cur == kHashEmpty) {
-                const uint32_t e = atomicAdd(&d.ctr->numNew, 1u);
-                if (e < d.newCap) {
-                    d.hashNew[e] = slot;
-                } else {
-                    atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
-                    d.ctr->hashNeedsClear = 1u;
-                }
+                listNewCell(d, atomicAdd(&d.ctr->numNew, 1u), slot);
                 cur = key;
             }
         }
@@ -498,11 +509,28 @@ __device__ void hashInsert(const Dev& d, unsigned long long key, unsigned long l
     d.ctr->hashNeedsClear = 1u;
 }
 
+__device__ __forceinline__ uint32_t cellAt(uint32_t x28, uint32_t y28, uint32_t z28, uint32_t level) {
+    const uint32_t sh = (uint32_t)kMaxDepth + 1u - level;
+    return ((x28 >> sh) & 127u) + ((y28 >> sh) & 127u) * 128u + ((z28 >> sh) & 127u) * 16384u;
+}
+
+constexpr uint32_t kInsertGroup = 4;  // table updates a lane keeps in flight
+
 // voxelSampling (remolod_octree.cu:677-740) + sampleVoxel's test (:95-119):
 // every (point, level) pair whose cell bit was clear before this batch is a
 // candidate; the table keeps, per cell, the lowest global point index reaching
 // it (or the first to arrive). Bits are not written here, so every pair sees
 // the pre-batch grid, and the set of new cells is exactly the reference's.
+//
+// Latency, not bandwidth, bounds this kernel, so it runs as three phases of
+// independent memory operations instead of a chain per level: (1) the grid
+// words of every level at once (the ancestor row replaces the root-to-leaf
+// pointer chase); (2) per level, one leader per run of equal cells in the warp
+// (batch points ascend in index with the lane, so a run's first lane holds its
+// lowest index; spilled points use a full match); (3) each lane's table
+// updates in groups: all slot reads, then all claims, then all minimum
+// updates, with one new-cell counter bump per warp and group. A slot already
+// holding a lower index is left alone.
 __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restrict__ pts, uint32_t n) {
     const Counters* c = d.ctr;
     if (c->batchStop) return;
@@ -510,65 +538,161 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
     const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
-    const uint32_t stride = gridDim.x * blockDim.x;
+    // the expand loop stopped at its pass limit: a point's recorded leaf may
+    // have been split after its last count, so finish its descent
+    const bool mayBeStale = c->iter > d.maxExpandIters;
+    const bool lowest = d.voxelMode == 0u;
     const uint32_t lane = laneId();
-    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    const uint32_t per = (((total + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
+    const uint32_t begin = min(total, blockIdx.x * per), end = min(total, begin + per);
+    for (uint32_t base = begin; base < end; base += blockDim.x) {
         const uint32_t i = base + threadIdx.x;
-        bool active = i < total;
+        const bool active = i < end;
         Point p = {0.f, 0.f, 0.f, 0u};
-        uint32_t gidx = 0;
-        if (i < n) {
+        uint32_t gidx = 0, leaf = 0;
+        if (active && i < n) {
             p = loadPoint(pts + i);
             gidx = firstIndex + i;
+            leaf = d.leafOf[i];
         } else if (active) {
             p = d.spillPts[i - n];
             gidx = d.spillIdx[i - n];
+            leaf = d.spillLeaf[i - n];
         }
-        uint32_t x20 = 0, y20 = 0, z20 = 0, x28 = 0, y28 = 0, z28 = 0;
+        uint32_t x28 = 0, y28 = 0, z28 = 0, lv = 0;
         if (active) {
             x28 = quant28(p.x, d.boxMin[0], d.octreeSize);
             y28 = quant28(p.y, d.boxMin[1], d.octreeSize);
             z28 = quant28(p.z, d.boxMin[2], d.octreeSize);
-            // 2^28 d / size is 2^8 times 2^20 d / size exactly (power-of-two
-            // scaling commutes with round-to-nearest), so the 20-bit coordinate
-            // is the 28-bit one shifted; only a saturated conversion differs
-            x20 = x28 < 0xFFFFFF00u ? x28 >> 8 : quant20(p.x, d.boxMin[0], d.octreeSize);
-            y20 = y28 < 0xFFFFFF00u ? y28 >> 8 : quant20(p.y, d.boxMin[1], d.octreeSize);
-            z20 = z28 < 0xFFFFFF00u ? z28 >> 8 : quant20(p.z, d.boxMin[2], d.octreeSize);
+            lv = d.level[leaf];
+            if (mayBeStale) {
+                const uint32_t x20 = quant20(p.x, d.boxMin[0], d.octreeSize),
+                               y20 = quant20(p.y, d.boxMin[1], d.octreeSize),
+                               z20 = quant20(p.z, d.boxMin[2], d.octreeSize);
+                while (lv < (uint32_t)kMaxDepth) {
+                    const int32_t nx = d.child[leaf * 8u + childIndex(x20, y20, z20, lv)];
+                    if (nx < 0) break;
+                    leaf = (uint32_t)nx;
+                    lv += 1u;
+                }
+            }
         }
-        uint32_t cur = 0;
-        for (uint32_t level = 0; level < (uint32_t)kMaxDepth; level++) {
-            if (!__any_sync(0xFFFFFFFFu, active)) break;
+        // (1) which levels' cells were empty before this batch
+        const uint2* row = d.anc + (size_t)leaf * kMaxDepth;
+        uint32_t mask = 0;
+        for (uint32_t l0 = 0; l0 < (uint32_t)kMaxDepth; l0 += 8u) {
+            if (!__any_sync(0xFFFFFFFFu, active && lv > l0)) break;
+            uint2 a[8];
+#pragma unroll
+            for (uint32_t k = 0; k < 8u; k++)
+                a[k] = (active && l0 + k < lv) ? row[l0 + k] : make_uint2(kNone, kNone);
+            uint32_t w[8];
+#pragma unroll
+            for (uint32_t k = 0; k < 8u; k++) {
+                w[k] = ~0u;
+                if (a[k].y != kNone)
+                    w[k] = __ldg(gridWordsAt(d, a[k].y) + (cellAt(x28, y28, z28, l0 + k) >> 5));
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < 8u; k++)
+                if (((w[k] >> (cellAt(x28, y28, z28, l0 + k) & 31u)) & 1u) == 0u) mask |= 1u << (l0 + k);
+        }
+        // the point's own node samples too while it has a grid (a root that has never split)
+        if (active) {
+            const uint32_t g = d.grid[leaf];
+            if (g != kNone) {
+                const uint32_t vi = cellAt(x28, y28, z28, lv);
+                if (((__ldg(gridWordsAt(d, g) + (vi >> 5)) >> (vi & 31u)) & 1u) == 0u) mask |= 1u << lv;
+            }
+        }
+        // (2) the levels this lane updates the table for
+        const bool ordered = __all_sync(0xFFFFFFFFu, !active || i < n);
+        uint32_t lead = 0;
+        uint32_t todo = __reduce_or_sync(0xFFFFFFFFu, mask);
+        while (todo) {
+            const uint32_t l = (uint32_t)(__ffs(todo) - 1);
+            todo &= todo - 1u;
             unsigned long long key = kHashEmpty;
-            if (active) {
-                const uint32_t g = __ldg(&d.grid[cur]);
-                if (g != kNone) {
-                    const uint32_t sh = (uint32_t)kMaxDepth + 1u - level;
-                    const uint32_t px = (x28 >> sh) & 127u, py = (y28 >> sh) & 127u,
-                                   pz = (z28 >> sh) & 127u;
-                    const uint32_t vi = px + py * 128u + pz * 16384u;
-                    const uint32_t word = __ldg(gridWordsAt(d, g) + (vi >> 5));
-                    if ((word & (1u << (vi & 31u))) == 0u)
-                        key = ((unsigned long long)cur << 21) | (unsigned long long)vi;
-                }
-                const int32_t nx = __ldg(&d.child[cur * 8u + childIndex(x20, y20, z20, level)]);
-                if (nx < 0) active = false;
-                else cur = (uint32_t)nx;
+            if ((mask >> l) & 1u) {
+                const uint32_t node = l < lv ? row[l].x : leaf;
+                key = ((unsigned long long)node << 21) | (unsigned long long)cellAt(x28, y28, z28, l);
             }
-            // most levels of a warp hold no new cell: skip the match there
-            if (!__any_sync(0xFFFFFFFFu, key != kHashEmpty)) continue;
-            const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
-            if (key != kHashEmpty) {
-                int leader;
-                if (d.voxelMode == 0u) {
-                    const uint32_t mn = __reduce_min_sync(peers, gidx);
-                    leader = (gidx == mn) ? (int)lane : -1;
-                } else {
-                    leader = (lane == (uint32_t)(__ffs(peers) - 1)) ? (int)lane : -1;
-                }
-                if (leader == (int)lane)
-                    hashInsert(d, key, ((unsigned long long)gidx << 32) | p.color);
+            bool first;
+            if (ordered) {
+                const unsigned long long prev = __shfl_up_sync(0xFFFFFFFFu, key, 1);
+                first = key != kHashEmpty && (lane == 0u || prev != key);
+            } else {
+                const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+                if (lowest) first = key != kHashEmpty && gidx == __reduce_min_sync(peers, gidx);
+                else first = key != kHashEmpty && lane == (uint32_t)(__ffs(peers) - 1);
             }
+            if (first) lead |= 1u << l;
+        }
+        // (3) table updates, kInsertGroup levels at a time
+        const unsigned long long val = ((unsigned long long)gidx << 32) | p.color;
+        while (__any_sync(0xFFFFFFFFu, lead != 0u)) {
+            unsigned long long key[kInsertGroup];
+            uint32_t slot[kInsertGroup];
+            uint32_t nk = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < kInsertGroup; j++) {
+                key[j] = kHashEmpty;
+                slot[j] = 0;
+                if (lead) {
+                    const uint32_t l = (uint32_t)(__ffs(lead) - 1);
+                    lead &= lead - 1u;
+                    const uint32_t node = l < lv ? row[l].x : leaf;
+                    key[j] = ((unsigned long long)node << 21) | (unsigned long long)cellAt(x28, y28, z28, l);
+                    slot[j] = hashSlot(key[j], d.hashMask);
+                    nk = j + 1u;
+                }
+            }
+            ulonglong2 kv[kInsertGroup];
+#pragma unroll
+            for (uint32_t j = 0; j < kInsertGroup; j++)
+                kv[j] = j < nk ? __ldcg(&d.hashSlots[slot[j]]) : make_ulonglong2(kHashEmpty, 0ull);
+            // 0: settled, 1: update the value, 2: claim the slot, 3: probe further
+            uint32_t state[kInsertGroup];
+            unsigned long long got[kInsertGroup];
+#pragma unroll
+            for (uint32_t j = 0; j < kInsertGroup; j++) {
+                state[j] = 0u;
+                got[j] = kHashEmpty;
+                if (j < nk) {
+                    if (kv[j].x == key[j]) state[j] = (lowest ? kv[j].y > val : kv[j].y == kHashEmpty) ? 1u : 0u;
+                    else if (kv[j].x == kHashEmpty) state[j] = 2u;
+                    else state[j] = 3u;
+                }
+                if (state[j] == 2u) got[j] = atomicCAS(&d.hashSlots[slot[j]].x, kHashEmpty, key[j]);
+            }
+            uint32_t claimed = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < kInsertGroup; j++) {
+                if (state[j] == 2u) {
+                    if (got[j] == kHashEmpty) claimed |= 1u << j;
+                    state[j] = (got[j] == kHashEmpty || got[j] == key[j]) ? 1u : 3u;
+                }
+                if (state[j] == 1u) {
+                    if (lowest) atomicMin(&d.hashSlots[slot[j]].y, val);
+                    else atomicCAS(&d.hashSlots[slot[j]].y, kHashEmpty, val);
+                } else if (state[j] == 3u) {
+                    hashInsertFrom(d, key[j], val, (slot[j] + 1u) & d.hashMask);
+                }
+            }
+            // one counter bump per warp for the slots claimed in this group
+            const uint32_t nc = (uint32_t)__popc(claimed);
+            uint32_t pre = nc;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, pre, o);
+                if (lane >= (uint32_t)o) pre += y;
+            }
+            uint32_t e0 = 0;
+            if (lane == 31u && pre) e0 = atomicAdd(&d.ctr->numNew, pre);
+            e0 = __shfl_sync(0xFFFFFFFFu, e0, 31) + pre - nc;
+#pragma unroll
+            for (uint32_t j = 0; j < kInsertGroup; j++)
+                if ((claimed >> j) & 1u) listNewCell(d, e0++, slot[j]);
         }
     }
 }

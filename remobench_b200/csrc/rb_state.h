@@ -119,9 +119,9 @@ struct SplitRec {
     uint32_t tableOff;      // its point chunk table (kept readable for the copy)
     uint32_t spillBase;     // first spill slot of its points
     uint32_t chunkBase;     // first copy work item
-    uint32_t numChunks;
+    uint32_t numChunks;     // chunks it owned (copy and recycle work items)
     uint32_t grid;
-    uint32_t pad;
+    uint32_t queueBase;     // chunk-queue position of its first recycled chunk, kNone: none
 };
 
 // Exact integer sums of one node (see rb_accum.cu).

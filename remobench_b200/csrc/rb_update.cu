@@ -82,6 +82,59 @@ __device__ __forceinline__ unsigned long long globalTimerNs() {
 // memory check, and for device-driven builds the batch cursor -- which slot
 // holds batch batchletIndex and how many points it has -- and the call's time
 // budget. A stopped batch leaves every later phase kernel a no-op.
+// Adds g points to a leaf's counter and lists the leaf when its count first
+// passes the split limit (the same test as countAt).
+__device__ __forceinline__ void addCount(const Dev& d, uint32_t leaf, uint32_t g) {
+    const uint32_t old = atomicAdd(&d.counter[leaf], g);
+    if (old <= d.maxPointsPerNode && old + g > d.maxPointsPerNode) {
+        const uint32_t k = atomicAdd(&d.ctr->numSpill, 1u);
+        if (k < d.spillingCap) d.spillNodes[k] = leaf;
+        else atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfSpilling);
+    }
+}
+
+// Block-level counting: the points of one block's contiguous range fall into
+// a handful of leaves, so counts are merged per block in shared memory and
+// each leaf's counter takes one atomic per block instead of one per warp (a
+// few hot counters otherwise serialise thousands of atomics). The final sums
+// and the set of leaves crossing the limit are the same.
+constexpr uint32_t kBlockLeaves = 64;
+
+struct BlockCounts {
+    uint32_t leaf[kBlockLeaves];
+    uint32_t cnt[kBlockLeaves];
+};
+
+__device__ __forceinline__ void blockCountsInit(BlockCounts& b) {
+    for (uint32_t t = threadIdx.x; t < kBlockLeaves; t += blockDim.x) {
+        b.leaf[t] = kNone;
+        b.cnt[t] = 0;
+    }
+}
+
+// Every lane of the warp calls it; lanes with nothing to count pass kNone.
+__device__ __forceinline__ void blockCountAt(const Dev& d, BlockCounts& b, uint32_t leaf) {
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, leaf);
+    if (leaf == kNone || (int)laneId() != __ffs(peers) - 1) return;
+    const uint32_t g = __popc(peers);
+    uint32_t slot = (leaf * 0x9E3779B1u) >> 26;
+    for (uint32_t probe = 0; probe < 8u; probe++) {
+        const uint32_t cur = atomicCAS(&b.leaf[slot], kNone, leaf);
+        if (cur == kNone || cur == leaf) {
+            atomicAdd(&b.cnt[slot], g);
+            return;
+        }
+        slot = (slot + 1u) & (kBlockLeaves - 1u);
+    }
+    addCount(d, leaf, g);  // crowded table: count globally
+}
+
+// After a barrier: the block's sums into the leaves' counters.
+__device__ __forceinline__ void blockCountsFlush(const Dev& d, BlockCounts& b) {
+    for (uint32_t t = threadIdx.x; t < kBlockLeaves; t += blockDim.x)
+        if (b.leaf[t] != kNone && b.cnt[t] != 0u) addCount(d, b.leaf[t], b.cnt[t]);
+}
+
 __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     Counters* c = d.ctr;
     uint32_t reason = 0;
@@ -156,22 +209,29 @@ __global__ void k_expand_cond(Dev d, cudaGraphConditionalHandle h) {
         }                                                               \
     } while (0)
 
+// Each block takes one contiguous, warp-aligned range of the batch.
 __global__ void __launch_bounds__(256) k_count_first(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    __shared__ BlockCounts s_counts;
     if (d.ctr->batchStop) return;
     RB_BATCH_AT_CURSOR(d, pts, n);
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    blockCountsInit(s_counts);
+    __syncthreads();
+    const uint32_t per = (((n + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
+    const uint32_t begin = min(n, blockIdx.x * per), end = min(n, begin + per);
+    for (uint32_t base = begin; base < end; base += blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         uint32_t leaf = kNone;
-        if (i < n) {
+        if (i < end) {
             const Point p = loadPoint(pts + i);
             leaf = descendFromRoot(d, quant20(p.x, d.boxMin[0], d.octreeSize),
                                    quant20(p.y, d.boxMin[1], d.octreeSize),
                                    quant20(p.z, d.boxMin[2], d.octreeSize));
             d.leafOf[i] = leaf;
         }
-        countAt(d, leaf);
+        blockCountAt(d, s_counts, leaf);
     }
+    __syncthreads();
+    blockCountsFlush(d, s_counts);
 }
 
 // Iterations 2.. of expand. The reference re-descends every batch and spilled
@@ -200,19 +260,24 @@ __global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict_
         prevStamp = d.ctr->lastStamp;
     }
     RB_BATCH_AT_CURSOR(d, pts, n);
+    __shared__ BlockCounts s_counts;
+    blockCountsInit(s_counts);
+    __syncthreads();
     const uint32_t ns = d.ctr->numSpilled < d.spillCap ? d.ctr->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    const uint32_t per = (((total + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
+    const uint32_t begin = min(total, blockIdx.x * per), end = min(total, begin + per);
+    for (uint32_t base = begin; base < end; base += blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         uint32_t leaf = kNone;
-        if (i < n) {
+        if (i >= end) {
+        } else if (i < n) {
             const uint32_t cur = d.leafOf[i];
             if (d.splitIter[cur] == prevStamp) {
                 leaf = stepIfSplit(d, cur, loadPoint(pts + i), prevStamp);
                 if (leaf != kNone) d.leafOf[i] = leaf;
             }
-        } else if (i < total) {
+        } else {
             const uint32_t j = i - n;
             const uint32_t cur = d.spillLeaf[j];
             if (d.splitIter[cur] == prevStamp) {
@@ -220,8 +285,10 @@ __global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict_
                 if (leaf != kNone) d.spillLeaf[j] = leaf;
             }
         }
-        if (__any_sync(0xFFFFFFFFu, leaf != kNone)) countAt(d, leaf);
+        if (__any_sync(0xFFFFFFFFu, leaf != kNone)) blockCountAt(d, s_counts, leaf);
     }
+    __syncthreads();
+    blockCountsFlush(d, s_counts);
 }
 
 // Block-wide exclusive scan of one value per thread (blockDim.x == 1024).
@@ -319,20 +386,17 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
     __syncthreads();
     for (uint32_t k0 = 0; k0 < acc; k0 += blockDim.x) {
         const uint32_t k = k0 + threadIdx.x;
-        uint32_t node = 0, np = 0, nch = 0;
+        uint32_t node = 0, np = 0, owned = 0;
         if (k < acc) {
             node = list[k];
-            const uint32_t cap = d.numPointChunks[node] * d.ppc;
+            owned = d.numPointChunks[node];
+            const uint32_t cap = owned * d.ppc;
             np = d.numPoints[node] < cap ? d.numPoints[node] : cap;
-            nch = (np + d.ppc - 1) / d.ppc;
         }
         uint32_t totPts, totCh;
         const uint32_t prePts = blockExclusiveScan(np, &totPts, s_warp);
-        const uint32_t preCh = blockExclusiveScan(nch, &totCh, s_warp);
+        const uint32_t preCh = blockExclusiveScan(owned, &totCh, s_warp);
         if (k < acc) {
-            const uint32_t base = nn + 8u * k;
-            const uint32_t lv = d.level[node] + 1u;
-            const uint32_t X = d.nodeX[node], Y = d.nodeY[node], Z = d.nodeZ[node];
             uint32_t g = d.grid[node];
             if (g == kNone) {
                 g = arenaAlloc(d, kGridUnits);
@@ -341,35 +405,6 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
                 atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
                           (unsigned long long)refAllocSize(kGridBytes));
             }
-            const uint2* prow = d.anc + (size_t)node * kMaxDepth;
-            for (uint32_t i = 0; i < 8; i++) {
-                const uint32_t ch = base + i;
-#pragma unroll
-                for (int q = 0; q < 8; q++) d.child[ch * 8u + q] = -1;
-                d.counter[ch] = 0;
-                d.numPoints[ch] = 0;
-                d.level[ch] = lv;
-                d.nodeX[ch] = 2u * X + ((i >> 2) & 1u);
-                d.nodeY[ch] = 2u * Y + ((i >> 1) & 1u);
-                d.nodeZ[ch] = 2u * Z + (i & 1u);
-                d.grid[ch] = kNone;
-                d.numVoxels[ch] = 0;
-                d.numVoxelsStored[ch] = 0;
-                d.numPointChunks[ch] = 0;
-                d.numVoxelChunks[ch] = 0;
-                d.ptTableOff[ch] = kNone;
-                d.ptTableCap[ch] = 0;
-                d.vxTableOff[ch] = kNone;
-                d.vxTableCap[ch] = 0;
-                d.splitIter[ch] = 0;
-                d.dirtyStamp[ch] = 0;
-                AccumI z = {};
-                d.accum[ch] = z;
-                uint2* crow = d.anc + (size_t)ch * kMaxDepth;
-                for (uint32_t l = 0; l + 1u < lv; l++) crow[l] = prow[l];
-                crow[lv - 1u] = make_uint2(node, g);
-                d.child[node * 8u + i] = (int32_t)ch;
-            }
             d.splitIter[node] = stamp;
             SplitRec r;
             r.node = node;
@@ -377,14 +412,10 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
             r.tableOff = d.ptTableOff[node];
             r.spillBase = spilledBefore + s_runPts + prePts;
             r.chunkBase = s_runChunks + preCh;
-            r.numChunks = nch;
-            // chunks go back to the queue (remolod_octree.cu:349-360)
-            const uint32_t owned = d.numPointChunks[node];
-            if (owned) {
-                const uint32_t base0 = atomicSub(&c->numAllocatedChunks, owned) - owned;
-                for (uint32_t j = 0; j < owned; j++)
-                    if (base0 + j < d.maxPtChunks) d.chunkQueue[base0 + j] = d.tablePool[r.tableOff + j];
-            }
+            r.numChunks = owned;
+            // the node's chunks go back to the queue (remolod_octree.cu:349-360);
+            // k_spill_copy writes them at these positions, one per work item
+            r.queueBase = owned ? atomicSub(&c->numAllocatedChunks, owned) - owned : kNone;
             d.numPoints[node] = 0;
             d.numPointChunks[node] = 0;
             d.ptTableOff[node] = kNone;
@@ -404,6 +435,40 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
         }
         __syncthreads();
     }
+    // the children: one thread each, the next 8 ids after the pool's end per node
+    for (uint32_t t = threadIdx.x; t < 8u * acc; t += blockDim.x) {
+        const uint32_t k = t >> 3, i = t & 7u;
+        const SplitRec r = d.splitRecs[k];
+        const uint32_t node = r.node;
+        const uint32_t ch = nn + t;
+        const uint32_t lv = d.level[node] + 1u;
+#pragma unroll
+        for (int q = 0; q < 8; q++) d.child[ch * 8u + q] = -1;
+        d.counter[ch] = 0;
+        d.numPoints[ch] = 0;
+        d.level[ch] = lv;
+        d.nodeX[ch] = 2u * d.nodeX[node] + ((i >> 2) & 1u);
+        d.nodeY[ch] = 2u * d.nodeY[node] + ((i >> 1) & 1u);
+        d.nodeZ[ch] = 2u * d.nodeZ[node] + (i & 1u);
+        d.grid[ch] = kNone;
+        d.numVoxels[ch] = 0;
+        d.numVoxelsStored[ch] = 0;
+        d.numPointChunks[ch] = 0;
+        d.numVoxelChunks[ch] = 0;
+        d.ptTableOff[ch] = kNone;
+        d.ptTableCap[ch] = 0;
+        d.vxTableOff[ch] = kNone;
+        d.vxTableCap[ch] = 0;
+        d.splitIter[ch] = 0;
+        d.dirtyStamp[ch] = 0;
+        AccumI z = {};
+        d.accum[ch] = z;
+        const uint2* prow = d.anc + (size_t)node * kMaxDepth;
+        uint2* crow = d.anc + (size_t)ch * kMaxDepth;
+        for (uint32_t l = 0; l + 1u < lv; l++) crow[l] = prow[l];
+        crow[lv - 1u] = make_uint2(node, r.grid);
+        d.child[node * 8u + i] = (int32_t)ch;
+    }
     if (threadIdx.x == 0) {
         c->numNodes = nn + 8u * acc;
         c->numSplit = acc;
@@ -421,9 +486,10 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
     }
 }
 
-// The split nodes' stored points move to the spill list (remolod_octree.cu:250-285)
-// and their grids are zeroed (:372-387). Work items: one per stored chunk, then
-// one per grid. Any grid size; items are strided over blocks.
+// The split nodes' stored points move to the spill list (remolod_octree.cu:250-285),
+// their chunks return to the queue (:349-360) and their grids are zeroed
+// (:372-387). Work items: one per owned chunk, then one per grid. Any grid
+// size; items are strided over blocks.
 __global__ void __launch_bounds__(256) k_spill_copy(Dev d) {
     const Counters* c = d.ctr;
     if (c->batchStop) return;
@@ -442,6 +508,7 @@ __global__ void __launch_bounds__(256) k_spill_copy(Dev d) {
             const SplitRec r = d.splitRecs[lo];
             const uint32_t j = w - r.chunkBase;
             const uint32_t phys = d.tablePool[r.tableOff + j];
+            if (threadIdx.x == 0 && r.queueBase + j < d.maxPtChunks) d.chunkQueue[r.queueBase + j] = phys;
             if (phys == kNone) continue;
             const uint32_t first = j * d.ppc;
             uint32_t last = first + d.ppc;

@@ -135,6 +135,58 @@ __device__ __forceinline__ void blockCountsFlush(const Dev& d, BlockCounts& b) {
         if (b.leaf[t] != kNone && b.cnt[t] != 0u) addCount(d, b.leaf[t], b.cnt[t]);
 }
 
+// Block-level slot reservation: each item takes the next slot of its key's
+// counter (a leaf's point count, a node's voxel count). Items of one block
+// merge per key in shared memory, so each key's counter takes one atomic per
+// block and pass instead of one per warp. Every thread of the block calls it
+// with its key (kNone: no item); it returns the item's slot.
+struct BlockSlots {
+    uint32_t key[kBlockLeaves];
+    uint32_t cnt[kBlockLeaves];
+    uint32_t base[kBlockLeaves];
+};
+
+__device__ __forceinline__ void blockSlotsInit(BlockSlots& b) {
+    for (uint32_t t = threadIdx.x; t < kBlockLeaves; t += blockDim.x) {
+        b.key[t] = kNone;
+        b.cnt[t] = 0;
+    }
+}
+
+__device__ __forceinline__ uint32_t blockReserve(BlockSlots& b, uint32_t* counters, uint32_t key) {
+    const uint32_t lane = laneId();
+    const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    uint32_t s = kNone, off = 0;
+    if (key != kNone && (int)lane == leader) {
+        const uint32_t g = __popc(peers);
+        uint32_t h = (key * 0x9E3779B1u) >> 26;
+        for (uint32_t probe = 0; probe < 8u; probe++) {
+            const uint32_t cur = atomicCAS(&b.key[h], kNone, key);
+            if (cur == kNone || cur == key) {
+                s = h;
+                off = atomicAdd(&b.cnt[h], g);
+                break;
+            }
+            h = (h + 1u) & (kBlockLeaves - 1u);
+        }
+        if (s == kNone) off = atomicAdd(&counters[key], g);  // crowded table: reserve globally
+    }
+    s = __shfl_sync(0xFFFFFFFFu, s, leader);
+    off = __shfl_sync(0xFFFFFFFFu, off, leader);
+    __syncthreads();
+    // one global reservation per key; the table empties for the next pass
+    // (the next pass writes base only after its own first barrier)
+    for (uint32_t t = threadIdx.x; t < kBlockLeaves; t += blockDim.x) {
+        if (b.key[t] != kNone) b.base[t] = atomicAdd(&counters[b.key[t]], b.cnt[t]);
+        b.key[t] = kNone;
+        b.cnt[t] = 0;
+    }
+    __syncthreads();
+    return key == kNone ? kNone : (s != kNone ? b.base[s] : 0u) + off + rank;
+}
+
 __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     Counters* c = d.ctr;
     uint32_t reason = 0;
@@ -767,14 +819,18 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
 // Sets the new cells' bits and gives each new voxel its slot in its node
 // (sampleVoxel :119-138). Keys are unique, so every bit is set exactly once.
 __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
+    __shared__ BlockSlots s_slots;
     const Counters* c = d.ctr;
     if (c->batchStop) return;
+    blockSlotsInit(s_slots);
+    __syncthreads();
     const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
-    const uint32_t lane = laneId();
-    for (uint32_t base = blockIdx.x * blockDim.x; base < nnew; base += gridDim.x * blockDim.x) {
+    const uint32_t per = (((nnew + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
+    const uint32_t begin = min(nnew, blockIdx.x * per), end = min(nnew, begin + per);
+    for (uint32_t base = begin; base < end; base += blockDim.x) {
         const uint32_t e = base + threadIdx.x;
         uint32_t node = kNone;
-        if (e < nnew) {
+        if (e < end) {
             // the table is final here: move the cell out of it and free the slot
             const uint32_t slot = d.hashNew[e];
             const ulonglong2 kv = d.hashSlots[slot];
@@ -786,14 +842,8 @@ __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
             d.hashNewCell[e] = vi;
             d.hashNewColor[e] = (uint32_t)(kv.y & 0xFFFFFFFFull);
         }
-        // one counter bump per warp and node
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, node);
-        if (node == kNone) continue;
-        const int leader = __ffs(peers) - 1;
-        uint32_t b0 = 0;
-        if ((int)lane == leader) b0 = atomicAdd(&d.numVoxels[node], (uint32_t)__popc(peers));
-        b0 = __shfl_sync(peers, b0, leader);
-        d.hashNewSlot[e] = b0 + __popc(peers & ((1u << lane) - 1u));
+        const uint32_t s = blockReserve(s_slots, d.numVoxels, node);
+        if (node != kNone) d.hashNewSlot[e] = s;
     }
 }
 
@@ -898,36 +948,35 @@ __global__ void __launch_bounds__(256) k_alloc_chunks(Dev d) {
 // insertPoints (remolod_octree.cu:794-883): batch points, then spilled points,
 // each into the leaf expand left it in. Slots are handed out per warp and leaf.
 __global__ void __launch_bounds__(256) k_insert(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    __shared__ BlockSlots s_slots;
     Counters* c = d.ctr;
     if (c->batchStop) return;
     RB_BATCH_AT_CURSOR(d, pts, n);
+    blockSlotsInit(s_slots);
+    __syncthreads();
     const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t lane = laneId();
     const uint32_t ppc = d.ppc;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < total; base += stride) {
+    const uint32_t per = (((total + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
+    const uint32_t begin = min(total, blockIdx.x * per), end = min(total, begin + per);
+    for (uint32_t base = begin; base < end; base += blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         uint32_t leaf = kNone, gidx = 0;
         Point p = {0.f, 0.f, 0.f, 0u};
-        if (i < n) {
+        if (i >= end) {
+        } else if (i < n) {
             leaf = d.leafOf[i];
             p = loadPoint(pts + i);
             gidx = firstIndex + i;
-        } else if (i < total) {
+        } else {
             const uint32_t j = i - n;
             leaf = d.spillLeaf[j];
             p = d.spillPts[j];
             gidx = d.spillIdx[j];
         }
-        const unsigned peers = __match_any_sync(0xFFFFFFFFu, leaf);
+        const uint32_t slot = blockReserve(s_slots, d.numPoints, leaf);
         if (leaf == kNone) continue;
-        const int leader = __ffs(peers) - 1;
-        uint32_t slotBase = 0;
-        if ((int)lane == leader) slotBase = atomicAdd(&d.numPoints[leaf], (uint32_t)__popc(peers));
-        slotBase = __shfl_sync(peers, slotBase, leader);
-        const uint32_t slot = slotBase + __popc(peers & ((1u << lane) - 1u));
         const uint32_t cap = d.numPointChunks[leaf] * ppc;
         uint32_t phys = kNone;
         if (slot < cap) phys = d.tablePool[d.ptTableOff[leaf] + slot / ppc];

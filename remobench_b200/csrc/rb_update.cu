@@ -634,6 +634,22 @@ __device__ __forceinline__ uint32_t cellAt(uint32_t x28, uint32_t y28, uint32_t 
 }
 
 constexpr uint32_t kInsertGroup = 4;  // table updates a lane keeps in flight
+// Per-warp buffer of claimed table slots: under 32 waiting plus one group of
+// at most 32 lanes x kInsertGroup claims.
+constexpr uint32_t kWarpCells = 32u + 32u * kInsertGroup;
+
+// The warp's buffered slots into the batch's list of new cells, with one
+// counter atomic (a single counter bumped by every claim serialises the
+// claims of the whole grid). Every lane of the warp calls it.
+__device__ __forceinline__ void flushWarpCells(const Dev& d, const uint32_t* wbuf, uint32_t count) {
+    if (count == 0u) return;
+    const uint32_t lane = laneId();
+    uint32_t e0 = 0;
+    if (lane == 0u) e0 = atomicAdd(&d.ctr->numNew, count);
+    e0 = __shfl_sync(0xFFFFFFFFu, e0, 0);
+    for (uint32_t t = lane; t < count; t += 32u) listNewCell(d, e0 + t, wbuf[t]);
+    __syncwarp();
+}
 
 // voxelSampling (remolod_octree.cu:677-740) + sampleVoxel's test (:95-119):
 // every (point, level) pair whose cell bit was clear before this batch is a
@@ -651,9 +667,12 @@ constexpr uint32_t kInsertGroup = 4;  // table updates a lane keeps in flight
 // updates, with one new-cell counter bump per warp and group. A slot already
 // holding a lower index is left alone.
 __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    __shared__ uint32_t s_wbuf[256 / 32][kWarpCells];
     const Counters* c = d.ctr;
     if (c->batchStop) return;
     RB_BATCH_AT_CURSOR(d, pts, n);
+    uint32_t* wbuf = s_wbuf[threadIdx.x >> 5];
+    uint32_t wbufN = 0;  // the same in every lane of the warp
     const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
@@ -798,7 +817,8 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
                     hashInsertFrom(d, key[j], val, (slot[j] + 1u) & d.hashMask);
                 }
             }
-            // one counter bump per warp for the slots claimed in this group
+            // the claimed slots wait in the warp's buffer; 32 or more go to the
+            // list of new cells with one counter atomic
             const uint32_t nc = (uint32_t)__popc(claimed);
             uint32_t pre = nc;
 #pragma unroll
@@ -806,14 +826,20 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
                 const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, pre, o);
                 if (lane >= (uint32_t)o) pre += y;
             }
-            uint32_t e0 = 0;
-            if (lane == 31u && pre) e0 = atomicAdd(&d.ctr->numNew, pre);
-            e0 = __shfl_sync(0xFFFFFFFFu, e0, 31) + pre - nc;
+            const uint32_t added = __shfl_sync(0xFFFFFFFFu, pre, 31);
+            uint32_t pos = wbufN + pre - nc;
 #pragma unroll
             for (uint32_t j = 0; j < kInsertGroup; j++)
-                if ((claimed >> j) & 1u) listNewCell(d, e0++, slot[j]);
+                if ((claimed >> j) & 1u) wbuf[pos++] = slot[j];
+            __syncwarp();
+            wbufN += added;
+            if (wbufN >= 32u) {
+                flushWarpCells(d, wbuf, wbufN);
+                wbufN = 0;
+            }
         }
     }
+    flushWarpCells(d, wbuf, wbufN);
 }
 
 // Sets the new cells' bits and gives each new voxel its slot in its node

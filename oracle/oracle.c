@@ -20,6 +20,9 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 #define OR_MAX_DEPTH 20
 #define OR_GRID_WORDS 65536u          /* 128^3 bits as 32-bit words (remolod_structures.cuh:66-68) */
@@ -64,6 +67,19 @@ struct or_tree {
 };
 
 /* ------------------------------------------------------------ helpers */
+
+/* Threads for the batch loops: cfg.num_threads (0 or 1: one). Every threaded
+ * loop either reads the tree only, or updates order-independent counters
+ * atomically; everything order-dependent stays sequential, so the result is
+ * the same for any thread count. */
+static int or_threads(const or_tree* t) {
+#ifdef _OPENMP
+    return t->cfg.num_threads > 1u ? (int)t->cfg.num_threads : 1;
+#else
+    (void)t;
+    return 1;
+#endif
+}
 
 /* cvt.rzi.sat.u32.f32: NaN and negatives to 0, saturating at 2^32-1. */
 static uint32_t cvt_u32(float v) {
@@ -273,7 +289,7 @@ static void count_point(count_ctx* cc, const or_point* p, uint32_t* fresh_tag) {
     uint32_t q20[3], q28[3];
     quantize(cc->t, p, q20, q28);
     uint32_t leaf = descend(cc->t, q20);
-    if (fresh_tag[leaf] < cc->iter_tag) cc->t->nodes[leaf].counter++;
+    if (fresh_tag[leaf] < cc->iter_tag) __atomic_fetch_add(&cc->t->nodes[leaf].counter, 1u, __ATOMIC_RELAXED);
 }
 
 /* expand (remolod_octree.cu:402-462) */
@@ -288,8 +304,12 @@ static void expand(or_tree* t, const or_point* pts, uint32_t n, uint32_t batch_i
         if (!before) abort();
         for (uint32_t i = 0; i < nn; i++) before[i] = t->nodes[i].counter;
         count_ctx cc = {t, iter_tag, before, NULL};
-        for (uint32_t i = 0; i < n; i++) count_point(&cc, &pts[i], fresh_tag);
-        for (uint64_t i = 0; i < t->spill_n; i++) count_point(&cc, &t->spill[i].p, fresh_tag);
+        const int nth = or_threads(t);
+        const int64_t nb = (int64_t)n, nsp = (int64_t)t->spill_n;
+#pragma omp parallel for num_threads(nth) schedule(static) if (nth > 1)
+        for (int64_t i = 0; i < nb; i++) count_point(&cc, &pts[i], fresh_tag);
+#pragma omp parallel for num_threads(nth) schedule(static) if (nth > 1)
+        for (int64_t i = 0; i < nsp; i++) count_point(&cc, &t->spill[i].p, fresh_tag);
         /* spilling nodes: the counter crossed the limit in this iteration (:213-218) */
         uint32_t* spilling = NULL;
         uint32_t ns = 0;
@@ -345,51 +365,108 @@ typedef struct vbacklog {
     uint64_t n, cap;
 } vbacklog;
 
-static void sample_path(or_tree* t, const or_point* p, vbacklog* bl) {
+/* A (point, level) pair whose cell bit was clear before the batch. */
+typedef struct vcand {
+    uint32_t node, vi, color;
+} vcand;
+
+typedef struct vcands {
+    vcand* v;
+    uint64_t n, cap;
+} vcands;
+
+/* The candidate cells of one point's path, root first (reads the tree only). */
+static void sample_candidates(const or_tree* t, const or_point* p, vcands* out) {
     uint32_t q20[3], q28[3];
     quantize(t, p, q20, q28);
     uint32_t cur = 0;
     for (int level = 0; level < OR_MAX_DEPTH; level++) {
-        onode* n = &t->nodes[cur];
+        const onode* n = &t->nodes[cur];
         if (n->grid >= 0) {
             const uint32_t sh = (uint32_t)(OR_MAX_DEPTH + 1 - (int)n->level);
             uint32_t px = (q28[0] >> sh) % 128u;
             uint32_t py = (q28[1] >> sh) % 128u;
             uint32_t pz = (q28[2] >> sh) % 128u;
             uint32_t vi = px + py * 128u + pz * 16384u;
-            uint32_t* w = &t->grids[n->grid][vi / 32u];
-            uint32_t bit = 1u << (vi % 32u);
-            if ((*w & bit) == 0u) {
-                *w |= bit;
-                n->num_voxels++;
-                float node_size = t->octree_size / ldexpf(1.0f, (int)n->level);
-                float mnx = fmaf((float)n->X, node_size, t->box_min[0]);
-                float mny = fmaf((float)n->Y, node_size, t->box_min[1]);
-                float mnz = fmaf((float)n->Z, node_size, t->box_min[2]);
-                or_point v;
-                v.x = mnx + node_size * ((float)px + 0.5f) / 128.0f;
-                v.y = mny + node_size * ((float)py + 0.5f) / 128.0f;
-                v.z = mnz + node_size * ((float)pz + 0.5f) / 128.0f;
-                v.color = p->color;
-                if (bl->n >= OR_BACKLOG_CAPACITY) t->st.overflow_flags |= OR_OVERFLOW_BACKLOG;
-                else {
-                    if (bl->n == bl->cap) {
-                        uint64_t cap = bl->cap ? 2 * bl->cap : 65536;
-                        voxel_new* nv = (voxel_new*)realloc(bl->v, cap * sizeof(voxel_new));
-                        if (!nv) abort();
-                        bl->v = nv;
-                        bl->cap = cap;
-                    }
-                    bl->v[bl->n].node = cur;
-                    bl->v[bl->n].v = v;
-                    bl->n++;
+            if ((t->grids[n->grid][vi / 32u] & (1u << (vi % 32u))) == 0u) {
+                if (out->n == out->cap) {
+                    uint64_t cap = out->cap ? 2 * out->cap : 4096;
+                    vcand* nv = (vcand*)realloc(out->v, cap * sizeof(vcand));
+                    if (!nv) abort();
+                    out->v = nv;
+                    out->cap = cap;
                 }
+                out->v[out->n].node = cur;
+                out->v[out->n].vi = vi;
+                out->v[out->n].color = p->color;
+                out->n++;
             }
         }
         int32_t c = n->child[child_index(q20, level)];
         if (c < 0) break;
         cur = (uint32_t)c;
     }
+}
+
+/* sampleVoxel's commit in visiting order: the first candidate of a cell sets
+ * its bit and makes the voxel, at the cell centre with its colour. */
+static void sample_commit(or_tree* t, const vcand* cd, vbacklog* bl) {
+    onode* n = &t->nodes[cd->node];
+    uint32_t* w = &t->grids[n->grid][cd->vi / 32u];
+    uint32_t bit = 1u << (cd->vi % 32u);
+    if (*w & bit) return;
+    *w |= bit;
+    n->num_voxels++;
+    const uint32_t px = cd->vi % 128u, py = (cd->vi / 128u) % 128u, pz = cd->vi / 16384u;
+    float node_size = t->octree_size / ldexpf(1.0f, (int)n->level);
+    float mnx = fmaf((float)n->X, node_size, t->box_min[0]);
+    float mny = fmaf((float)n->Y, node_size, t->box_min[1]);
+    float mnz = fmaf((float)n->Z, node_size, t->box_min[2]);
+    or_point v;
+    v.x = mnx + node_size * ((float)px + 0.5f) / 128.0f;
+    v.y = mny + node_size * ((float)py + 0.5f) / 128.0f;
+    v.z = mnz + node_size * ((float)pz + 0.5f) / 128.0f;
+    v.color = cd->color;
+    if (bl->n >= OR_BACKLOG_CAPACITY) {
+        t->st.overflow_flags |= OR_OVERFLOW_BACKLOG;
+        return;
+    }
+    if (bl->n == bl->cap) {
+        uint64_t cap = bl->cap ? 2 * bl->cap : 65536;
+        voxel_new* nv = (voxel_new*)realloc(bl->v, cap * sizeof(voxel_new));
+        if (!nv) abort();
+        bl->v = nv;
+        bl->cap = cap;
+    }
+    bl->v[bl->n].node = cd->node;
+    bl->v[bl->n].v = v;
+    bl->n++;
+}
+
+/* voxelSampling over the visiting order (spilled points by original index,
+ * then the batch): candidates per contiguous range in parallel, committed in
+ * order, which is the sequential result. */
+static void sample_all(or_tree* t, const or_point* pts, uint32_t n, vbacklog* bl) {
+    const int nth = or_threads(t);
+    const uint64_t total = t->spill_n + n;
+    vcands* parts = (vcands*)calloc((size_t)nth, sizeof(vcands));
+    if (!parts) abort();
+#pragma omp parallel num_threads(nth) if (nth > 1)
+    {
+        int tid = 0, tn = 1;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+        tn = omp_get_num_threads();
+#endif
+        const uint64_t lo = total * (uint64_t)tid / (uint64_t)tn, hi = total * (uint64_t)(tid + 1) / (uint64_t)tn;
+        for (uint64_t i = lo; i < hi; i++)
+            sample_candidates(t, i < t->spill_n ? &t->spill[i].p : &pts[i - t->spill_n], &parts[tid]);
+    }
+    for (int k = 0; k < nth; k++) {
+        for (uint64_t i = 0; i < parts[k].n; i++) sample_commit(t, &parts[k].v[i], bl);
+        free(parts[k].v);
+    }
+    free(parts);
 }
 
 static void ensure_pts_cap(onode* n, uint32_t cap) {
@@ -452,10 +529,14 @@ static void alloc_voxel_chunks(or_tree* t) {
 }
 
 /* insertPoints' per-point body (remolod_octree.cu:804-860) */
-static void insert_point(or_tree* t, const or_point* p, uint32_t index) {
+static uint32_t leaf_of(const or_tree* t, const or_point* p) {
     uint32_t q20[3], q28[3];
     quantize(t, p, q20, q28);
-    onode* n = &t->nodes[descend(t, q20)];
+    return descend(t, q20);
+}
+
+static void insert_at(or_tree* t, uint32_t leaf, const or_point* p, uint32_t index) {
+    onode* n = &t->nodes[leaf];
     uint32_t slot = n->num_points++;
     uint32_t cap = n->num_point_chunks * t->cfg.points_per_chunk;
     if (slot >= cap) {
@@ -488,14 +569,23 @@ int or_add_batch(or_tree* t, const or_point* pts, uint32_t n) {
     /* spilled points in increasing original index, then the batch in order */
     qsort(t->spill, t->spill_n, sizeof(spill_pt), cmp_spill);
     vbacklog bl = {NULL, 0, 0};
-    for (uint64_t i = 0; i < t->spill_n; i++) sample_path(t, &t->spill[i].p, &bl);
-    for (uint32_t i = 0; i < n; i++) sample_path(t, &pts[i], &bl);
+    sample_all(t, pts, n, &bl);
 
     alloc_point_chunks(t);
     alloc_voxel_chunks(t);
 
-    for (uint32_t i = 0; i < n; i++) insert_point(t, &pts[i], first_index + i);
-    for (uint64_t i = 0; i < t->spill_n; i++) insert_point(t, &t->spill[i].p, t->spill[i].index);
+    /* insertPoints: leaves in parallel (the tree is fixed now), slots in order */
+    const uint64_t total = (uint64_t)n + t->spill_n;
+    uint32_t* leaves = (uint32_t*)malloc((size_t)(total ? total : 1) * sizeof(uint32_t));
+    if (!leaves) abort();
+    const int nth = or_threads(t);
+    const int64_t tot = (int64_t)total;
+#pragma omp parallel for num_threads(nth) schedule(static) if (nth > 1)
+    for (int64_t i = 0; i < tot; i++)
+        leaves[i] = leaf_of(t, i < (int64_t)n ? &pts[i] : &t->spill[i - (int64_t)n].p);
+    for (uint32_t i = 0; i < n; i++) insert_at(t, leaves[i], &pts[i], first_index + i);
+    for (uint64_t i = 0; i < t->spill_n; i++) insert_at(t, leaves[n + i], &t->spill[i].p, t->spill[i].index);
+    free(leaves);
 
     /* insertVoxels (remolod_octree.cu:918-938) */
     for (uint64_t i = 0; i < bl.n; i++) {

@@ -206,3 +206,25 @@ def test_jacobi_known_eigenvalues():
     a = np.array([[4.0, 1.0, 0.5], [1.0, 3.0, 0.2], [0.5, 0.2, 1.0]])
     e, _ = ob.sym3_eig([a[0, 0], a[0, 1], a[0, 2], a[1, 1], a[1, 2], a[2, 2]])
     assert np.allclose(e, np.sort(np.linalg.eigvalsh(a))[::-1], rtol=1e-12)
+
+
+def test_threaded_builder_matches_sequential(c1_cloud):
+    """The multithreaded CPU builder (the timed CPU baseline) builds the same
+    tree, points and voxels, in the same order, as the sequential one."""
+    cfg, cloud, bmin, bmax = c1_cloud
+    sub = cloud[: 4 * cfg.batch_size]
+    trees = []
+    for threads in (1, 4):
+        t = ob.Tree(num_threads=threads)
+        t.reset(bmin, bmax)
+        for b in range(4):
+            assert t.add_batch(sub[b * cfg.batch_size:(b + 1) * cfg.batch_size]) == 0
+        t.sweep()
+        trees.append(t)
+    a, b = trees
+    assert np.array_equal(a.node_table(), b.node_table())
+    for i in range(a.num_nodes()):
+        pa, ia = a.leaf_points(i)
+        pb, ib = b.leaf_points(i)
+        assert np.array_equal(ia, ib) and np.array_equal(pa.view(np.uint32), pb.view(np.uint32))
+        assert np.array_equal(a.node_voxels(i).view(np.uint32), b.node_voxels(i).view(np.uint32))

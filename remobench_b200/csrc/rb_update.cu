@@ -1200,7 +1200,7 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         cudaGraph_t bodyOut = nullptr;
         if ((e = cudaStreamEndCapture(bs, &bodyOut)) != cudaSuccess) break;
         k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
-        k_vox_commit<<<fixedGrid, 256, 0, cs>>>(d);
+        k_vox_commit<<<pointGrid, 256, 0, cs>>>(d);
         k_alloc_chunks<<<fixedGrid, 256, 0, cs>>>(d);
         k_insert<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         k_vox_store<<<fixedGrid, 256, 0, cs>>>(d);

@@ -1,5 +1,6 @@
-// Accumulate stage: per-leaf running sums behind a watermark, one block per
-// dirty leaf (restates kernels/remolod/remolod_accum.cu:47-233).
+// Accumulate stage: per-leaf running sums behind a watermark, restating
+// kernels/remolod/remolod_accum.cu:47-233. A plan splits every dirty leaf's
+// new points into fixed-size work items spread over the whole grid.
 //
 // The reference sums node-local coordinates in [0, 1] as doubles, so its sums
 // depend on the order the points are folded in. Here each point is quantised
@@ -50,31 +51,126 @@ __device__ __forceinline__ bool leafRow(const Dev& d, uint32_t node) {
 constexpr int kAccumThreads = 256;
 constexpr int kAccumWarps = kAccumThreads / 32;
 constexpr int kNumSums = 3 + 12 + 3 + 3;  // s1, s2 (lo, hi), c1, c2
+// Points per work item: a leaf's new range is split over several blocks, so
+// a fold over a few hundred big leaves still fills the GPU.
+constexpr uint32_t kAccumChunk = 4096;
 
-// Folds one leaf's [count, numPoints) or clears an inner node's sums.
-// useList: iterate the dirty list; otherwise every node.
-__global__ void __launch_bounds__(kAccumThreads) k_accumulate(Dev d, uint32_t batchIndex, int useList) {
+// 128-bit atomic add on a (lo, hi) pair: the add that wraps lo carries into hi.
+__device__ __forceinline__ void atomicAdd128(unsigned long long* lo, unsigned long long* hi,
+                                             unsigned long long vlo, unsigned long long vhi) {
+    const unsigned long long old = atomicAdd(lo, vlo);
+    const unsigned long long carry = (old + vlo < old) ? 1ull : 0ull;
+    if (vhi + carry) atomicAdd(hi, vhi + carry);
+}
+
+// The fold's plan (one block): the nodes to visit (the dirty list, or every
+// node), each leaf's new range [count, min(numPoints, capacity)) read before
+// any block updates count, and each node's first work item. An inner node
+// with sums is one item (cleared); a leaf with new points one item per
+// kAccumChunk points. Folded-leaf and point totals are counted here.
+__global__ void __launch_bounds__(1024) k_accum_plan(Dev d, int useList) {
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_run, s_leaves;
+    __shared__ unsigned long long s_points;
+    Counters* c = d.ctr;
+    const uint32_t total = useList ? (c->numDirty < d.maxNodes ? c->numDirty : d.maxNodes) : c->numNodes;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        s_run = 0;
+        s_leaves = 0;
+        s_points = 0;
+    }
+    __syncthreads();
+    for (uint32_t w0 = 0; w0 < total; w0 += blockDim.x) {
+        const uint32_t w = w0 + threadIdx.x;
+        uint32_t items = 0, from = 0, to = 0;
+        if (w < total) {
+            const uint32_t node = useList ? d.dirtyList[w] : w;
+            if (!leafRow(d, node)) {
+                items = d.accum[node].count != 0u ? 1u : 0u;
+            } else {
+                from = d.accum[node].count;
+                const uint32_t cap = d.numPointChunks[node] * d.ppc;
+                const uint32_t np = d.numPoints[node];
+                to = np < cap ? np : cap;
+                if (to > from) {
+                    items = (to - from + kAccumChunk - 1u) / kAccumChunk;
+                    atomicAdd(&s_leaves, 1u);
+                    atomicAdd(&s_points, (unsigned long long)(to - from));
+                } else {
+                    to = from;
+                }
+            }
+            d.accumFrom[w] = from;
+            d.accumTo[w] = to;
+        }
+        // block-wide exclusive scan of the item counts
+        uint32_t x = items;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        if (lane == 31u) s_warp[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t v = lane < blockDim.x / 32u ? s_warp[lane] : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+                if (lane >= (uint32_t)o) v += y;
+            }
+            s_warp[lane] = v;
+        }
+        __syncthreads();
+        const uint32_t pre = s_run + (warp > 0 ? s_warp[warp - 1] : 0u) + x - items;
+        if (w < total) d.accumItem[w] = pre;
+        __syncthreads();
+        if (threadIdx.x == 0) s_run += s_warp[blockDim.x / 32u - 1u];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        d.accumItem[total] = s_run;
+        c->accumItems = s_run;
+        d.accumGlobals->numAccumulated += s_points;
+        d.accumGlobals->pointsFolded += (uint32_t)s_points;
+        d.accumGlobals->numLeavesFolded += s_leaves;
+    }
+}
+
+// Folds the plan's work items: each a kAccumChunk-point slice of one leaf's
+// new range (partial sums added atomically into the leaf's exact sums; any
+// order gives the same bits), or an inner node's sums cleared.
+__global__ void __launch_bounds__(kAccumThreads, 4) k_accumulate(Dev d, uint32_t batchIndex, int useList) {
     __shared__ unsigned long long s_red[kNumSums][kAccumWarps];
     __shared__ unsigned long long s_morton[kAccumWarps];
     const Counters* c = d.ctr;
     const uint32_t total = useList ? (c->numDirty < d.maxNodes ? c->numDirty : d.maxNodes) : c->numNodes;
+    const uint32_t items = c->accumItems;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t ppc = d.ppc;
-    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+    for (uint32_t it = blockIdx.x; it < items; it += gridDim.x) {
+        // the node whose items hold this one: last w with accumItem[w] <= it
+        uint32_t lo = 0, hi = total;
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (d.accumItem[mid] <= it) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t w = lo;
         const uint32_t node = useList ? d.dirtyList[w] : w;
         AccumI* a = &d.accum[node];
-        if (!leafRow(d, node)) {
-            if (threadIdx.x == 0 && a->count != 0) {
+        const uint32_t from0 = d.accumFrom[w], to = d.accumTo[w];
+        if (to == from0) {  // an inner node holding sums
+            if (threadIdx.x == 0) {
                 AccumI z = {};
                 *a = z;
             }
             continue;
         }
-        const uint32_t from = a->count;
-        const uint32_t to = d.numPoints[node];
-        if (to <= from) continue;
-        const uint32_t cap = d.numPointChunks[node] * ppc;
-        const uint32_t end = to < cap ? to : cap;
+        const uint32_t k0 = it - d.accumItem[w];
+        const uint32_t from = from0 + k0 * kAccumChunk;
+        const uint32_t end = min(to, from + kAccumChunk);
         const uint32_t lv = d.level[node];
         const uint32_t sh = 28u - lv;
         const long long lim = 1ll << sh;
@@ -83,44 +179,75 @@ __global__ void __launch_bounds__(kAccumThreads) k_accumulate(Dev d, uint32_t ba
         const long long bz = (long long)d.nodeZ[node] << sh;
         const uint32_t toff = d.ptTableOff[node];
 
+        // Per thread at most kAccumChunk / kAccumThreads = 16 points per item:
+        // Σq < 2^32 · 16 needs u64, Σq·q < 16 · 2^56 fits u64 without carries,
+        // colour sums fit u32; the 128-bit carries start at the warp reduction.
         unsigned long long s1[3] = {0, 0, 0};
-        unsigned long long lo[6] = {0, 0, 0, 0, 0, 0}, hi[6] = {0, 0, 0, 0, 0, 0};
-        unsigned long long c1[3] = {0, 0, 0}, c2[3] = {0, 0, 0};
+        unsigned long long p2[6] = {0, 0, 0, 0, 0, 0};
+        uint32_t c1[3] = {0, 0, 0}, c2[3] = {0, 0, 0};
         unsigned long long wm = 0;
-        for (uint32_t s = from + threadIdx.x; s < end; s += blockDim.x) {
-            const uint32_t phys = d.tablePool[toff + s / ppc];
-            if (phys == kNone) continue;
-            const float4 v = __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc));
-            const uint32_t P[3] = {aq(v.x, d.boxMin[0], d.octreeSize, 268435456.0f),
-                                   aq(v.y, d.boxMin[1], d.octreeSize, 268435456.0f),
-                                   aq(v.z, d.boxMin[2], d.octreeSize, 268435456.0f)};
-            long long q[3] = {(long long)P[0] - bx, (long long)P[1] - by, (long long)P[2] - bz};
+        for (uint32_t s0 = from + threadIdx.x; s0 < end; s0 += 2u * blockDim.x) {
+            // two points per step: independent chunk-table and point loads in flight
+            float4 v2[2];
+            bool ok[2];
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-                q[k] = q[k] < 0 ? 0 : (q[k] > lim ? lim : q[k]);
-                s1[k] += (unsigned long long)q[k];
+            for (int h = 0; h < 2; h++) {
+                const uint32_t s = s0 + (uint32_t)h * blockDim.x;
+                ok[h] = false;
+                if (s < end) {
+                    const uint32_t phys = d.tablePool[toff + s / ppc];
+                    if (phys != kNone) {
+                        v2[h] = __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc));
+                        ok[h] = true;
+                    }
+                }
             }
-            add128(lo[0], hi[0], (unsigned long long)(q[0] * q[0]));
-            add128(lo[1], hi[1], (unsigned long long)(q[0] * q[1]));
-            add128(lo[2], hi[2], (unsigned long long)(q[0] * q[2]));
-            add128(lo[3], hi[3], (unsigned long long)(q[1] * q[1]));
-            add128(lo[4], hi[4], (unsigned long long)(q[1] * q[2]));
-            add128(lo[5], hi[5], (unsigned long long)(q[2] * q[2]));
-            const uint32_t col = __float_as_uint(v.w);
-            const uint32_t ch[3] = {col & 255u, (col >> 8) & 255u, (col >> 16) & 255u};
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-                c1[k] += ch[k];
-                c2[k] += ch[k] * ch[k];
+            for (int h = 0; h < 2; h++) {
+                if (!ok[h]) continue;
+                const float4 v = v2[h];
+                const uint32_t P[3] = {aq(v.x, d.boxMin[0], d.octreeSize, 268435456.0f),
+                                       aq(v.y, d.boxMin[1], d.octreeSize, 268435456.0f),
+                                       aq(v.z, d.boxMin[2], d.octreeSize, 268435456.0f)};
+                long long q[3] = {(long long)P[0] - bx, (long long)P[1] - by, (long long)P[2] - bz};
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    q[k] = q[k] < 0 ? 0 : (q[k] > lim ? lim : q[k]);
+                    s1[k] += (unsigned long long)q[k];
+                }
+                p2[0] += (unsigned long long)(q[0] * q[0]);
+                p2[1] += (unsigned long long)(q[0] * q[1]);
+                p2[2] += (unsigned long long)(q[0] * q[2]);
+                p2[3] += (unsigned long long)(q[1] * q[1]);
+                p2[4] += (unsigned long long)(q[1] * q[2]);
+                p2[5] += (unsigned long long)(q[2] * q[2]);
+                const uint32_t col = __float_as_uint(v.w);
+                const uint32_t ch[3] = {col & 255u, (col >> 8) & 255u, (col >> 16) & 255u};
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    c1[k] += ch[k];
+                    c2[k] += ch[k] * ch[k];
+                }
+                // the 20-bit coordinate is the 28-bit one shifted (power-of-two scaling
+                // commutes with round-to-nearest); only a saturated conversion differs
+                uint32_t X = P[0] < 0xFFFFFF00u ? P[0] >> 8 : aq(v.x, d.boxMin[0], d.octreeSize, 1048576.0f);
+                uint32_t Y = P[1] < 0xFFFFFF00u ? P[1] >> 8 : aq(v.y, d.boxMin[1], d.octreeSize, 1048576.0f);
+                uint32_t Z = P[2] < 0xFFFFFF00u ? P[2] >> 8 : aq(v.z, d.boxMin[2], d.octreeSize, 1048576.0f);
+                X = X < 1048575u ? X : 1048575u;
+                Y = Y < 1048575u ? Y : 1048575u;
+                Z = Z < 1048575u ? Z : 1048575u;
+                const unsigned long long m = (mortonSpread(X) << 2) | (mortonSpread(Y) << 1) | mortonSpread(Z);
+                wm = m > wm ? m : wm;
             }
-            uint32_t X = aq(v.x, d.boxMin[0], d.octreeSize, 1048576.0f);
-            uint32_t Y = aq(v.y, d.boxMin[1], d.octreeSize, 1048576.0f);
-            uint32_t Z = aq(v.z, d.boxMin[2], d.octreeSize, 1048576.0f);
-            X = X < 1048575u ? X : 1048575u;
-            Y = Y < 1048575u ? Y : 1048575u;
-            Z = Z < 1048575u ? Z : 1048575u;
-            const unsigned long long m = (mortonSpread(X) << 2) | (mortonSpread(Y) << 1) | mortonSpread(Z);
-            wm = m > wm ? m : wm;
+        }
+        unsigned long long lo2[6], hi2[6] = {0, 0, 0, 0, 0, 0};
+        unsigned long long c1w[3], c2w[3];
+#pragma unroll
+        for (int k = 0; k < 6; k++) lo2[k] = p2[k];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            c1w[k] = c1[k];
+            c2w[k] = c2[k];
         }
         // warp reduction
 #pragma unroll
@@ -128,16 +255,16 @@ __global__ void __launch_bounds__(kAccumThreads) k_accumulate(Dev d, uint32_t ba
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 s1[k] += __shfl_down_sync(0xFFFFFFFFu, s1[k], off);
-                c1[k] += __shfl_down_sync(0xFFFFFFFFu, c1[k], off);
-                c2[k] += __shfl_down_sync(0xFFFFFFFFu, c2[k], off);
+                c1w[k] += __shfl_down_sync(0xFFFFFFFFu, c1w[k], off);
+                c2w[k] += __shfl_down_sync(0xFFFFFFFFu, c2w[k], off);
             }
 #pragma unroll
             for (int k = 0; k < 6; k++) {
-                const unsigned long long ol = __shfl_down_sync(0xFFFFFFFFu, lo[k], off);
-                const unsigned long long oh = __shfl_down_sync(0xFFFFFFFFu, hi[k], off);
-                const unsigned long long nl = lo[k] + ol;
-                hi[k] += oh + (nl < lo[k] ? 1ull : 0ull);
-                lo[k] = nl;
+                const unsigned long long ol = __shfl_down_sync(0xFFFFFFFFu, lo2[k], off);
+                const unsigned long long oh = __shfl_down_sync(0xFFFFFFFFu, hi2[k], off);
+                const unsigned long long nl = lo2[k] + ol;
+                hi2[k] += oh + (nl < lo2[k] ? 1ull : 0ull);
+                lo2[k] = nl;
             }
             const unsigned long long om = __shfl_down_sync(0xFFFFFFFFu, wm, off);
             wm = om > wm ? om : wm;
@@ -145,38 +272,42 @@ __global__ void __launch_bounds__(kAccumThreads) k_accumulate(Dev d, uint32_t ba
         if (lane == 0) {
             for (int k = 0; k < 3; k++) {
                 s_red[k][warp] = s1[k];
-                s_red[15 + k][warp] = c1[k];
-                s_red[18 + k][warp] = c2[k];
+                s_red[15 + k][warp] = c1w[k];
+                s_red[18 + k][warp] = c2w[k];
             }
             for (int k = 0; k < 6; k++) {
-                s_red[3 + k][warp] = lo[k];
-                s_red[9 + k][warp] = hi[k];
+                s_red[3 + k][warp] = lo2[k];
+                s_red[9 + k][warp] = hi2[k];
             }
             s_morton[warp] = wm;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            AccumI acc = *a;
+            unsigned long long t1[3] = {0, 0, 0}, tc1[3] = {0, 0, 0}, tc2[3] = {0, 0, 0};
+            unsigned long long tlo[6] = {0, 0, 0, 0, 0, 0}, thi[6] = {0, 0, 0, 0, 0, 0};
             unsigned long long m = 0;
             for (int w2 = 0; w2 < kAccumWarps; w2++) {
                 for (int k = 0; k < 3; k++) {
-                    acc.s1[k] += s_red[k][w2];
-                    acc.c1[k] += s_red[15 + k][w2];
-                    acc.c2[k] += s_red[18 + k][w2];
+                    t1[k] += s_red[k][w2];
+                    tc1[k] += s_red[15 + k][w2];
+                    tc2[k] += s_red[18 + k][w2];
                 }
                 for (int k = 0; k < 6; k++) {
-                    acc.s2hi[k] += s_red[9 + k][w2];
-                    add128(acc.s2lo[k], acc.s2hi[k], s_red[3 + k][w2]);
+                    thi[k] += s_red[9 + k][w2];
+                    add128(tlo[k], thi[k], s_red[3 + k][w2]);
                 }
                 m = s_morton[w2] > m ? s_morton[w2] : m;
             }
-            acc.count = to;
-            acc.lastTouchedBatch = batchIndex;
-            *a = acc;
+            for (int k = 0; k < 3; k++) {
+                atomicAdd(&a->s1[k], t1[k]);
+                atomicAdd(&a->c1[k], tc1[k]);
+                atomicAdd(&a->c2[k], tc2[k]);
+            }
+            for (int k = 0; k < 6; k++) atomicAdd128(&a->s2lo[k], &a->s2hi[k], tlo[k], thi[k]);
+            // every item of a leaf writes the same watermark and batch
+            a->count = to;
+            a->lastTouchedBatch = batchIndex;
             atomicMax(&d.accumGlobals->mortonWatermark, m);
-            atomicAdd(&d.accumGlobals->numAccumulated, (unsigned long long)(to - from));
-            atomicAdd(&d.accumGlobals->pointsFolded, to - from);
-            atomicAdd(&d.accumGlobals->numLeavesFolded, 1u);
         }
         __syncthreads();
     }
@@ -196,6 +327,7 @@ __global__ void __launch_bounds__(256) k_accum_verify(Dev d) {
 }
 
 void launchAccumulate(const Dev& d, uint32_t batchIndex, int useList, int grid, cudaStream_t s) {
+    k_accum_plan<<<1, 1024, 0, s>>>(d, useList);
     k_accumulate<<<grid, kAccumThreads, 0, s>>>(d, batchIndex, useList);
 }
 void launchAccumVerify(const Dev& d, int grid, cudaStream_t s) { k_accum_verify<<<grid, 256, 0, s>>>(d); }

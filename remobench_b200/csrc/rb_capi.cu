@@ -536,6 +536,9 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.ring, 1, "ring descriptor");
     ALLOC(d.sweep, 1, "sweep stats");
     ALLOC(d.accumGlobals, 1, "accumulator globals");
+    ALLOC(d.accumFrom, N, "accumulate plan ranges");
+    ALLOC(d.accumTo, N, "accumulate plan ranges");
+    ALLOC(d.accumItem, (uint64_t)N + 1, "accumulate plan items");
     ALLOC(c->vis, N, "visible flags");
     ALLOC(c->large, N, "large flags");
     ALLOC(c->items, std::max<uint32_t>(cfg.drawlist_capacity, 1), "draw list");

@@ -79,7 +79,7 @@ struct Counters {
     uint32_t expandGuard;         // expand passes of this batch (loop bound)
     uint32_t hashNeedsClear;      // the cell table holds entries its list cannot name
     uint32_t callBatches;         // batches built since the build call began
-    uint32_t pad3;
+    uint32_t accumItems;          // work items of the current Accumulate launch
 };
 
 enum StopReason : uint32_t { kStopMemory = 1u, kStopNoBatch = 2u, kStopTime = 3u };
@@ -207,6 +207,10 @@ struct Dev {
     RingDesc* ring;
     SweepStats* sweep;
     AccumGlobals* accumGlobals;
+    // Accumulate's plan: per visited node, its point range and first work item
+    uint32_t* accumFrom;     // [maxNodes]
+    uint32_t* accumTo;       // [maxNodes]
+    uint32_t* accumItem;     // [maxNodes + 1] exclusive prefix of work items
     // capacities and constants
     uint32_t maxNodes;
     uint32_t maxPointsPerNode;

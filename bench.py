@@ -324,9 +324,14 @@ def main():
     upd = {k: v for k, v in prof.items() if v["timed"] > 0 and k not in ("k_reset_root",)}
     total_k = sum(v["ms"] for v in upd.values())
     top = max(upd.items(), key=lambda kv: kv[1]["ms"])
-    # algorithmic bytes of the dominant kernel per point handed to it
+    # algorithmic bytes of the dominant kernel per point handed to it: the point
+    # read (16 B), plus its leaf id (4 B) where one is written, plus the stored
+    # point and index (20 B) for insertion
     bytes_per_unit = {"k_vox_sample": 16.0, "k_count_first": 20.0, "k_insert": 16.0 + 4.0 + 20.0,
                       "k_recount": 4.0, "k_accumulate": 16.0}
+    # DRAM bytes (read + write) per launch from one ncu capture of the kernel on
+    # 1M-point batches of the same generator (profiles/k_vox_sample_config2_1M_batch.md)
+    ncu_traffic = {"k_vox_sample": 43.3e6}
     peak, peak_kind = peaks()
     roof = None
     if top[0] in bytes_per_unit and top[1]["units"] > 0:
@@ -334,7 +339,9 @@ def main():
         per_launch_bytes = bytes_per_unit[top[0]] * top[1]["units"] / top[1]["launches"]
         achieved = per_launch_bytes / (avg_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": top[0], "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 5), "peak_kind": peak_kind, "traffic": None,
+                "frac": round(achieved / peak, 5), "peak_kind": peak_kind,
+                "traffic": ncu_traffic.get(top[0]), "traffic_unit": "bytes per launch (ncu)",
+                "algorithmic_bytes_per_launch": round(per_launch_bytes),
                 "avg_launch_ms": round(avg_ms, 4), "share": round(top[1]["ms"] / total_k, 3)}
 
     cpu = None

@@ -27,7 +27,7 @@ enum KernelId : int {
     K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END, K_ACCUMULATE, K_ACCUM_VERIFY,
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
-    K_HASH_RESET, K_EXPAND_COND, K_NUM
+    K_HASH_RESET, K_EXPAND_COND, K_ZERO_GRIDS, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
@@ -35,7 +35,7 @@ static const char* const kKernelNames[K_NUM] = {
     "k_accumulate", "k_accum_verify", "k_sweep", "k_reset_root", "k_fb_clear", "k_node_flags",
     "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve", "k_roll_level", "k_analyze",
     "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam", "k_hash_reset",
-    "k_expand_cond"};
+    "k_expand_cond", "k_zero_grids"};
 
 struct Profiler {
     bool on = false;
@@ -236,6 +236,7 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
         LAUNCH(c, K_RECOUNT, n, rb::launchRecount(d, pts, n, stamp, pointGrid(c, n), s));
     }
     const uint64_t work = n;
+    LAUNCH(c, K_ZERO_GRIDS, 0, rb::launchZeroGrids(d, fixedGrid, s));
     LAUNCH(c, K_VOX_SAMPLE, n, rb::launchVoxSample(d, pts, n, pointGrid(c, work), s));
     LAUNCH(c, K_VOX_COMMIT, 0, rb::launchVoxCommit(d, c->numSMs * 8, s));
     LAUNCH(c, K_ALLOC_CHUNKS, 0, rb::launchAllocChunks(d, fixedGrid, s));
@@ -258,14 +259,14 @@ bool graphPath(rb_ctx* c) {
     return c->batchGraph != nullptr;
 }
 
-// Launches of one graph batch, for the per-kernel counts: ten fixed kernels
-// per batch, four per pass of the expand loop.
+// Launches of one graph batch, for the per-kernel counts: eleven fixed
+// kernels per batch, four per pass of the expand loop.
 void countGraphLaunches(rb_ctx* c, uint64_t batches, uint64_t itersBefore, uint64_t done, uint64_t points) {
     // each built batch adds 1 + (its split passes) to expandIters
     const uint64_t iters = c->hostCtr->expandIters;
     const uint64_t passes = iters >= itersBefore + done ? iters - itersBefore - done : 0u;
-    for (int k : {K_HASH_RESET, K_BATCH_BEGIN, K_COUNT_FIRST, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT,
-                  K_VOX_STORE, K_BATCH_END})
+    for (int k : {K_HASH_RESET, K_BATCH_BEGIN, K_COUNT_FIRST, K_ZERO_GRIDS, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS,
+                  K_INSERT, K_VOX_STORE, K_BATCH_END})
         c->prof.launches[k] += batches;
     c->prof.launches[K_EXPAND_COND] += batches + passes;
     for (int k : {K_SPLIT, K_SPILL_COPY, K_RECOUNT}) c->prof.launches[k] += passes;
@@ -539,6 +540,8 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.accumFrom, N, "accumulate plan ranges");
     ALLOC(d.accumTo, N, "accumulate plan ranges");
     ALLOC(d.accumItem, (uint64_t)N + 1, "accumulate plan items");
+    d.zeroCap = N / 8u + 1u;
+    ALLOC(d.zeroList, d.zeroCap, "grids to zero");
     ALLOC(c->vis, N, "visible flags");
     ALLOC(c->large, N, "large flags");
     ALLOC(c->items, std::max<uint32_t>(cfg.drawlist_capacity, 1), "draw list");

@@ -34,6 +34,7 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
 void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchRecount(const Dev& d, const Point* pts, uint32_t n, uint32_t prevStamp, int grid, cudaStream_t s);
 void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s);
+void launchZeroGrids(const Dev& d, int grid, cudaStream_t s);
 void launchSpillCopy(const Dev& d, int grid, cudaStream_t s);
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchVoxCommit(const Dev& d, int grid, cudaStream_t s);

@@ -80,6 +80,8 @@ struct Counters {
     uint32_t hashNeedsClear;      // the cell table holds entries its list cannot name
     uint32_t callBatches;         // batches built since the build call began
     uint32_t accumItems;          // work items of the current Accumulate launch
+    uint32_t numZero;             // grids of nodes split this batch, to zero after expand
+    uint32_t pad4;
 };
 
 enum StopReason : uint32_t { kStopMemory = 1u, kStopNoBatch = 2u, kStopTime = 3u };
@@ -211,6 +213,8 @@ struct Dev {
     uint32_t* accumFrom;     // [maxNodes]
     uint32_t* accumTo;       // [maxNodes]
     uint32_t* accumItem;     // [maxNodes + 1] exclusive prefix of work items
+    uint32_t* zeroList;      // [zeroCap] grids to zero after the expand loop
+    uint32_t zeroCap;
     // capacities and constants
     uint32_t maxNodes;
     uint32_t maxPointsPerNode;

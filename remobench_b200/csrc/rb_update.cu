@@ -227,6 +227,7 @@ __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     c->spillChunkTotal = 0;
     c->iter = 1;
     c->expandGuard = 0;
+    c->numZero = 0;
     c->hashNeedsClear = 0;  // k_hash_reset ran before this kernel
 }
 
@@ -400,10 +401,17 @@ constexpr uint32_t kSortSmem = 8192;
 // in increasing node id, each taking the next block of 8 ids. One block of
 // 1024 threads: the list is short (14 nodes per batch on the reference's
 // 36M cloud, wiki/03_ExpandStageFindings.md:63).
+// per split node, for its children (the first kSplitInfo nodes of a pass)
+struct SplitInfo {
+    uint32_t node, lv, X, Y, Z, grid;
+};
+constexpr uint32_t kSplitInfo = 512;
+
 __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
     __shared__ uint32_t s_sort[kSortSmem];
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_runPts, s_runChunks;
+    __shared__ SplitInfo s_info[kSplitInfo];
     Counters* c = d.ctr;
     if (c->batchStop) return;
     // stamp 0: device-driven, (batch << 5) | pass as the host loop would pass it;
@@ -474,6 +482,22 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
             d.ptTableCap[node] = 0;
             r.grid = g;
             d.splitRecs[k] = r;
+            // its grid is zeroed after the expand loop (nothing reads it before
+            // voxel sampling), so passes without stored points copy nothing
+            if (g != kNone) {
+                const uint32_t z = atomicAdd(&c->numZero, 1u);
+                if (z < d.zeroCap) d.zeroList[z] = g;
+            }
+            if (k < kSplitInfo) {
+                SplitInfo info;
+                info.node = node;
+                info.lv = d.level[node];
+                info.X = d.nodeX[node];
+                info.Y = d.nodeY[node];
+                info.Z = d.nodeZ[node];
+                info.grid = g;
+                s_info[k] = info;
+            }
             if (d.dirtyStamp[node] != c->buildStamp) {
                 d.dirtyStamp[node] = c->buildStamp;
                 const uint32_t di = atomicAdd(&c->numDirty, 1u);
@@ -490,18 +514,28 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
     // the children: one thread each, the next 8 ids after the pool's end per node
     for (uint32_t t = threadIdx.x; t < 8u * acc; t += blockDim.x) {
         const uint32_t k = t >> 3, i = t & 7u;
-        const SplitRec r = d.splitRecs[k];
-        const uint32_t node = r.node;
+        SplitInfo info;
+        if (k < kSplitInfo) {
+            info = s_info[k];
+        } else {
+            info.node = d.splitRecs[k].node;
+            info.grid = d.splitRecs[k].grid;
+            info.lv = d.level[info.node];
+            info.X = d.nodeX[info.node];
+            info.Y = d.nodeY[info.node];
+            info.Z = d.nodeZ[info.node];
+        }
+        const uint32_t node = info.node;
         const uint32_t ch = nn + t;
-        const uint32_t lv = d.level[node] + 1u;
+        const uint32_t lv = info.lv + 1u;
 #pragma unroll
         for (int q = 0; q < 8; q++) d.child[ch * 8u + q] = -1;
         d.counter[ch] = 0;
         d.numPoints[ch] = 0;
         d.level[ch] = lv;
-        d.nodeX[ch] = 2u * d.nodeX[node] + ((i >> 2) & 1u);
-        d.nodeY[ch] = 2u * d.nodeY[node] + ((i >> 1) & 1u);
-        d.nodeZ[ch] = 2u * d.nodeZ[node] + (i & 1u);
+        d.nodeX[ch] = 2u * info.X + ((i >> 2) & 1u);
+        d.nodeY[ch] = 2u * info.Y + ((i >> 1) & 1u);
+        d.nodeZ[ch] = 2u * info.Z + (i & 1u);
         d.grid[ch] = kNone;
         d.numVoxels[ch] = 0;
         d.numVoxelsStored[ch] = 0;
@@ -517,8 +551,10 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
         d.accum[ch] = z;
         const uint2* prow = d.anc + (size_t)node * kMaxDepth;
         uint2* crow = d.anc + (size_t)ch * kMaxDepth;
-        for (uint32_t l = 0; l + 1u < lv; l++) crow[l] = prow[l];
-        crow[lv - 1u] = make_uint2(node, r.grid);
+#pragma unroll
+        for (uint32_t l = 0; l < (uint32_t)kMaxDepth; l++)
+            if (l + 1u < lv) crow[l] = prow[l];
+        crow[lv - 1u] = make_uint2(node, info.grid);
         d.child[node * 8u + i] = (int32_t)ch;
     }
     if (threadIdx.x == 0) {
@@ -538,18 +574,16 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
     }
 }
 
-// The split nodes' stored points move to the spill list (remolod_octree.cu:250-285),
-// their chunks return to the queue (:349-360) and their grids are zeroed
-// (:372-387). Work items: one per owned chunk, then one per grid. Any grid
-// size; items are strided over blocks.
+// The split nodes' stored points move to the spill list (remolod_octree.cu:250-285)
+// and their chunks return to the queue (:349-360): one work item per owned
+// chunk, strided over blocks.
 __global__ void __launch_bounds__(256) k_spill_copy(Dev d) {
     const Counters* c = d.ctr;
     if (c->batchStop) return;
     const uint32_t nsplit = c->numSplit;
     const uint32_t nchunk = c->spillChunkTotal;
-    const uint32_t items = nchunk + nsplit;
-    for (uint32_t w = blockIdx.x; w < items; w += gridDim.x) {
-        if (w < nchunk) {
+    for (uint32_t w = blockIdx.x; w < nchunk; w += gridDim.x) {
+        {
             // binary search for the record holding work item w
             uint32_t lo = 0, hi = nsplit;
             while (hi - lo > 1) {
@@ -572,13 +606,20 @@ __global__ void __launch_bounds__(256) k_spill_copy(Dev d) {
                 d.spillIdx[slot] = chunkIndices(d, phys)[s - first];
                 d.spillLeaf[slot] = r.node;
             }
-        } else {
-            const SplitRec r = d.splitRecs[w - nchunk];
-            if (r.grid == kNone) continue;
-            uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, r.grid));
-            const uint4 z = make_uint4(0, 0, 0, 0);
-            for (uint32_t q = threadIdx.x; q < kGridWords / 4u; q += blockDim.x) g[q] = z;
         }
+    }
+}
+
+// The grids of the nodes split in this batch, zeroed (:372-387) once after
+// the expand loop: one block per grid.
+__global__ void __launch_bounds__(256) k_zero_grids(Dev d) {
+    const Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t nz = c->numZero < d.zeroCap ? c->numZero : d.zeroCap;
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    for (uint32_t w = blockIdx.x; w < nz; w += gridDim.x) {
+        uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, d.zeroList[w]));
+        for (uint32_t q = threadIdx.x; q < kGridWords / 4u; q += blockDim.x) g[q] = z;
     }
 }
 
@@ -1136,6 +1177,7 @@ void launchRecount(const Dev& d, const Point* pts, uint32_t n, uint32_t prevStam
 }
 void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s) { k_split<<<1, 1024, 0, s>>>(d, stamp); }
 void launchSpillCopy(const Dev& d, int grid, cudaStream_t s) { k_spill_copy<<<grid, 256, 0, s>>>(d); }
+void launchZeroGrids(const Dev& d, int grid, cudaStream_t s) { k_zero_grids<<<grid, 256, 0, s>>>(d); }
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_vox_sample<<<grid, 256, 0, s>>>(d, pts, n);
 }
@@ -1199,6 +1241,7 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         k_expand_cond<<<1, 1, 0, bs>>>(d, h);
         cudaGraph_t bodyOut = nullptr;
         if ((e = cudaStreamEndCapture(bs, &bodyOut)) != cudaSuccess) break;
+        k_zero_grids<<<fixedGrid, 256, 0, cs>>>(d);
         k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         k_vox_commit<<<pointGrid, 256, 0, cs>>>(d);
         k_alloc_chunks<<<fixedGrid, 256, 0, cs>>>(d);

@@ -397,20 +397,91 @@ __device__ void bitonicSort(uint32_t* a, uint32_t n) {
 
 constexpr uint32_t kSortSmem = 8192;
 
-// doSplitting (remolod_octree.cu:303-400) for the nodes the last count found,
-// in increasing node id, each taking the next block of 8 ids. One block of
-// 1024 threads: the list is short (14 nodes per batch on the reference's
-// 36M cloud, wiki/03_ExpandStageFindings.md:63).
 // per split node, for its children (the first kSplitInfo nodes of a pass)
 struct SplitInfo {
     uint32_t node, lv, X, Y, Z, grid;
 };
 constexpr uint32_t kSplitInfo = 512;
 
+// Ascending bitonic sort of one value per lane.
+__device__ __forceinline__ uint32_t warpSortAscending(uint32_t v) {
+    const uint32_t lane = laneId();
+#pragma unroll
+    for (uint32_t k = 2; k <= 32u; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t o = __shfl_xor_sync(0xFFFFFFFFu, v, j);
+            const bool keepMin = ((lane & j) == 0u) == ((lane & k) == 0u);
+            v = keepMin ? min(v, o) : max(v, o);
+        }
+    }
+    return v;
+}
+
+// The bookkeeping of the k-th split node of a pass (remolod_octree.cu:303-400):
+// its grid, its split stamp, its record for the spill copy (spill slots and
+// copy items from the given prefixes), its chunks' queue positions, the grid
+// to zero, the dirty list; its fields for the children phase.
+__device__ __forceinline__ void splitBook(const Dev& d, Counters* c, uint32_t k, uint32_t node, uint32_t np,
+                                          uint32_t owned, uint32_t spillBase, uint32_t chunkBase, uint32_t stamp,
+                                          SplitInfo* s_info) {
+    uint32_t g = d.grid[node];
+    if (g == kNone) {
+        g = arenaAlloc(d, kGridUnits);
+        d.grid[node] = g;
+        atomicAdd(&c->numGrids, 1u);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset), (unsigned long long)refAllocSize(kGridBytes));
+    }
+    d.splitIter[node] = stamp;
+    SplitRec r;
+    r.node = node;
+    r.numPoints = np;
+    r.tableOff = d.ptTableOff[node];
+    r.spillBase = spillBase;
+    r.chunkBase = chunkBase;
+    r.numChunks = owned;
+    // the node's chunks go back to the queue (remolod_octree.cu:349-360);
+    // k_spill_copy writes them at these positions, one per work item
+    r.queueBase = owned ? atomicSub(&c->numAllocatedChunks, owned) - owned : kNone;
+    d.numPoints[node] = 0;
+    d.numPointChunks[node] = 0;
+    d.ptTableOff[node] = kNone;
+    d.ptTableCap[node] = 0;
+    r.grid = g;
+    d.splitRecs[k] = r;
+    // its grid is zeroed after the expand loop (nothing reads it before voxel
+    // sampling), so passes without stored points copy nothing
+    if (g != kNone) {
+        const uint32_t z = atomicAdd(&c->numZero, 1u);
+        if (z < d.zeroCap) d.zeroList[z] = g;
+    }
+    if (k < kSplitInfo) {
+        SplitInfo info;
+        info.node = node;
+        info.lv = d.level[node];
+        info.X = d.nodeX[node];
+        info.Y = d.nodeY[node];
+        info.Z = d.nodeZ[node];
+        info.grid = g;
+        s_info[k] = info;
+    }
+    if (d.dirtyStamp[node] != c->buildStamp) {
+        d.dirtyStamp[node] = c->buildStamp;
+        const uint32_t di = atomicAdd(&c->numDirty, 1u);
+        if (di < d.maxNodes) d.dirtyList[di] = node;
+    }
+}
+
+// doSplitting (remolod_octree.cu:303-400) for the nodes the last count found,
+// in increasing node id, each taking the next block of 8 ids. One block of
+// 1024 threads. Up to 32 spilling nodes (the usual case: 14 nodes per batch on
+// the reference's 36M cloud, wiki/03_ExpandStageFindings.md:63) are sorted,
+// scanned and booked by one warp with no block barrier; more go through a
+// block-wide sort and scans.
 __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
     __shared__ uint32_t s_sort[kSortSmem];
     __shared__ uint32_t s_warp[32];
-    __shared__ uint32_t s_runPts, s_runChunks;
+    __shared__ uint32_t s_runPts, s_runChunks, s_acc, s_nn;
     __shared__ SplitInfo s_info[kSplitInfo];
     Counters* c = d.ctr;
     if (c->batchStop) return;
@@ -423,93 +494,88 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
         if (threadIdx.x == 0) c->numSplit = 0;
         return;
     }
-    uint32_t* list;
-    if (ns <= kSortSmem) {
-        for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s_sort[i] = d.spillNodes[i];
-        __syncthreads();
-        bitonicSort(s_sort, ns);
-        list = s_sort;
-    } else {
-        // rare: sorts in the spilling-node buffer itself (sized to a power of two)
-        bitonicSort(d.spillNodes, ns);
-        list = d.spillNodes;
-    }
-    const uint32_t nn = c->numNodes;
-    const uint32_t room = d.maxNodes > nn ? (d.maxNodes - nn) / 8u : 0u;
-    const uint32_t acc = ns < room ? ns : room;
     const uint32_t spilledBefore = c->numSpilled;
-    if (threadIdx.x == 0) {
-        if (acc < ns) c->nodePoolOverflow = 1;
-        s_runPts = 0;
-        s_runChunks = 0;
-    }
-    __syncthreads();
-    for (uint32_t k0 = 0; k0 < acc; k0 += blockDim.x) {
-        const uint32_t k = k0 + threadIdx.x;
-        uint32_t node = 0, np = 0, owned = 0;
-        if (k < acc) {
-            node = list[k];
-            owned = d.numPointChunks[node];
-            const uint32_t cap = owned * d.ppc;
-            np = d.numPoints[node] < cap ? d.numPoints[node] : cap;
-        }
-        uint32_t totPts, totCh;
-        const uint32_t prePts = blockExclusiveScan(np, &totPts, s_warp);
-        const uint32_t preCh = blockExclusiveScan(owned, &totCh, s_warp);
-        if (k < acc) {
-            uint32_t g = d.grid[node];
-            if (g == kNone) {
-                g = arenaAlloc(d, kGridUnits);
-                d.grid[node] = g;
-                atomicAdd(&c->numGrids, 1u);
-                atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
-                          (unsigned long long)refAllocSize(kGridBytes));
+    uint32_t nn, acc;
+    if (ns <= 32u) {
+        if (threadIdx.x < 32u) {
+            const uint32_t lane = threadIdx.x;
+            const uint32_t node = warpSortAscending(lane < ns ? d.spillNodes[lane] : kNone);
+            const uint32_t n0 = c->numNodes;
+            const uint32_t room = d.maxNodes > n0 ? (d.maxNodes - n0) / 8u : 0u;
+            const uint32_t a = ns < room ? ns : room;
+            uint32_t np = 0, owned = 0;
+            if (lane < a) {
+                owned = d.numPointChunks[node];
+                const uint32_t cap = owned * d.ppc;
+                np = d.numPoints[node] < cap ? d.numPoints[node] : cap;
             }
-            d.splitIter[node] = stamp;
-            SplitRec r;
-            r.node = node;
-            r.numPoints = np;
-            r.tableOff = d.ptTableOff[node];
-            r.spillBase = spilledBefore + s_runPts + prePts;
-            r.chunkBase = s_runChunks + preCh;
-            r.numChunks = owned;
-            // the node's chunks go back to the queue (remolod_octree.cu:349-360);
-            // k_spill_copy writes them at these positions, one per work item
-            r.queueBase = owned ? atomicSub(&c->numAllocatedChunks, owned) - owned : kNone;
-            d.numPoints[node] = 0;
-            d.numPointChunks[node] = 0;
-            d.ptTableOff[node] = kNone;
-            d.ptTableCap[node] = 0;
-            r.grid = g;
-            d.splitRecs[k] = r;
-            // its grid is zeroed after the expand loop (nothing reads it before
-            // voxel sampling), so passes without stored points copy nothing
-            if (g != kNone) {
-                const uint32_t z = atomicAdd(&c->numZero, 1u);
-                if (z < d.zeroCap) d.zeroList[z] = g;
+            uint32_t xp = np, xc = owned;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t yp = __shfl_up_sync(0xFFFFFFFFu, xp, o);
+                const uint32_t yc = __shfl_up_sync(0xFFFFFFFFu, xc, o);
+                if (lane >= (uint32_t)o) {
+                    xp += yp;
+                    xc += yc;
+                }
             }
-            if (k < kSplitInfo) {
-                SplitInfo info;
-                info.node = node;
-                info.lv = d.level[node];
-                info.X = d.nodeX[node];
-                info.Y = d.nodeY[node];
-                info.Z = d.nodeZ[node];
-                info.grid = g;
-                s_info[k] = info;
-            }
-            if (d.dirtyStamp[node] != c->buildStamp) {
-                d.dirtyStamp[node] = c->buildStamp;
-                const uint32_t di = atomicAdd(&c->numDirty, 1u);
-                if (di < d.maxNodes) d.dirtyList[di] = node;
+            if (lane < a) splitBook(d, c, lane, node, np, owned, spilledBefore + xp - np, xc - owned, stamp, s_info);
+            const uint32_t totPts = __shfl_sync(0xFFFFFFFFu, xp, 31);
+            const uint32_t totCh = __shfl_sync(0xFFFFFFFFu, xc, 31);
+            if (lane == 0) {
+                if (a < ns) c->nodePoolOverflow = 1;
+                s_runPts = totPts;
+                s_runChunks = totCh;
+                s_acc = a;
+                s_nn = n0;
             }
         }
         __syncthreads();
+        acc = s_acc;
+        nn = s_nn;
+    } else {
+        uint32_t* list;
+        if (ns <= kSortSmem) {
+            for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s_sort[i] = d.spillNodes[i];
+            __syncthreads();
+            bitonicSort(s_sort, ns);
+            list = s_sort;
+        } else {
+            // rare: sorts in the spilling-node buffer itself (sized to a power of two)
+            bitonicSort(d.spillNodes, ns);
+            list = d.spillNodes;
+        }
+        nn = c->numNodes;
+        const uint32_t room = d.maxNodes > nn ? (d.maxNodes - nn) / 8u : 0u;
+        acc = ns < room ? ns : room;
         if (threadIdx.x == 0) {
-            s_runPts += totPts;
-            s_runChunks += totCh;
+            if (acc < ns) c->nodePoolOverflow = 1;
+            s_runPts = 0;
+            s_runChunks = 0;
         }
         __syncthreads();
+        for (uint32_t k0 = 0; k0 < acc; k0 += blockDim.x) {
+            const uint32_t k = k0 + threadIdx.x;
+            uint32_t node = 0, np = 0, owned = 0;
+            if (k < acc) {
+                node = list[k];
+                owned = d.numPointChunks[node];
+                const uint32_t cap = owned * d.ppc;
+                np = d.numPoints[node] < cap ? d.numPoints[node] : cap;
+            }
+            uint32_t totPts, totCh;
+            const uint32_t prePts = blockExclusiveScan(np, &totPts, s_warp);
+            const uint32_t preCh = blockExclusiveScan(owned, &totCh, s_warp);
+            if (k < acc)
+                splitBook(d, c, k, node, np, owned, spilledBefore + s_runPts + prePts, s_runChunks + preCh, stamp,
+                          s_info);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_runPts += totPts;
+                s_runChunks += totCh;
+            }
+            __syncthreads();
+        }
     }
     // the children: one thread each, the next 8 ids after the pool's end per node
     for (uint32_t t = threadIdx.x; t < 8u * acc; t += blockDim.x) {

@@ -78,6 +78,15 @@ def scene_box(cfg, relative=True):
     return (np.array(lo, dtype=np.float32), np.array(hi, dtype=np.float32))
 
 
+def scene_box_f64(cfg):
+    """(box_min, box_max) of the cloud in float64 world coordinates."""
+    info = SceneInfo()
+    if _load().rb_synth_scene_info_get(ctypes.byref(cfg), ctypes.byref(info)) != 0:
+        raise RuntimeError("scene construction failed")
+    return (np.array([float(v) for v in info.box_min], dtype=np.float64),
+            np.array([float(v) for v in info.box_max], dtype=np.float64))
+
+
 def generate(cfg, first=0, count=None, relative=True, out=None):
     """Points [first, first+count) as a structured float32/uint32 array."""
     if count is None:

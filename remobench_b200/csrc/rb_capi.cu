@@ -221,19 +221,21 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
     LAUNCH(c, K_BATCH_BEGIN, 1, rb::launchBatchBegin(d, s));
     LAUNCH(c, K_COUNT_FIRST, n, rb::launchCountFirst(d, pts, n, pointGrid(c, n), s));
     const int fixedGrid = c->numSMs * 4;
-    for (uint32_t iter = 1;; iter++) {
+    // the same kernels as the batch graph, with the loop test on the host;
+    // split and recount take their stamps from the device counters
+    LAUNCH(c, K_EXPAND_COND, 1, rb::launchExpandCond(d, s));
+    for (uint32_t pass = 0; pass < 64u; pass++) {
         rb_status st = readCounters(c);
         if (st != RB_OK) return st;
         if (c->hostCtr->batchStop) {
             *stopped = true;
             return RB_OK;
         }
-        if (c->hostCtr->numSpill == 0) break;
-        const uint32_t stamp = (batchIndex << 5) | iter;
-        LAUNCH(c, K_SPLIT, c->hostCtr->numSpill, rb::launchSplit(d, stamp, s));
+        if (c->hostCtr->numSpill == 0 || c->hostCtr->expandGuard > 40u) break;
+        LAUNCH(c, K_SPLIT, c->hostCtr->numSpill, rb::launchSplit(d, 0u, s));
         LAUNCH(c, K_SPILL_COPY, 0, rb::launchSpillCopy(d, fixedGrid, s));
-        if (iter >= c->cfg.max_expand_iters) break;
-        LAUNCH(c, K_RECOUNT, n, rb::launchRecount(d, pts, n, stamp, pointGrid(c, n), s));
+        LAUNCH(c, K_RECOUNT, n, rb::launchRecount(d, pts, n, 0u, pointGrid(c, n), s));
+        LAUNCH(c, K_EXPAND_COND, 1, rb::launchExpandCond(d, s));
     }
     const uint64_t work = n;
     LAUNCH(c, K_ZERO_GRIDS, 0, rb::launchZeroGrids(d, fixedGrid, s));
@@ -261,14 +263,15 @@ bool graphPath(rb_ctx* c) {
 
 // Launches of one graph batch, for the per-kernel counts: eleven fixed
 // kernels per batch, four per pass of the expand loop.
-void countGraphLaunches(rb_ctx* c, uint64_t batches, uint64_t itersBefore, uint64_t done, uint64_t points) {
-    // each built batch adds 1 + (its split passes) to expandIters
-    const uint64_t iters = c->hostCtr->expandIters;
-    const uint64_t passes = iters >= itersBefore + done ? iters - itersBefore - done : 0u;
+void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint64_t points) {
+    // every batch graph runs the loop test once after its first count and once
+    // after each split pass
+    const uint32_t conds = c->hostCtr->condRuns - condBefore;
+    const uint64_t passes = conds >= batches ? conds - batches : 0u;
     for (int k : {K_HASH_RESET, K_BATCH_BEGIN, K_COUNT_FIRST, K_ZERO_GRIDS, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS,
                   K_INSERT, K_VOX_STORE, K_BATCH_END})
         c->prof.launches[k] += batches;
-    c->prof.launches[K_EXPAND_COND] += batches + passes;
+    c->prof.launches[K_EXPAND_COND] += conds;
     for (int k : {K_SPLIT, K_SPILL_COPY, K_RECOUNT}) c->prof.launches[k] += passes;
     for (int k : {K_COUNT_FIRST, K_VOX_SAMPLE, K_INSERT}) c->prof.units[k] += points;
 }
@@ -540,6 +543,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.accumFrom, N, "accumulate plan ranges");
     ALLOC(d.accumTo, N, "accumulate plan ranges");
     ALLOC(d.accumItem, (uint64_t)N + 1, "accumulate plan items");
+    ALLOC(d.hist8, (uint64_t)N * 8, "child-octant counts");
     d.zeroCap = N / 8u + 1u;
     ALLOC(d.zeroList, d.zeroCap, "grids to zero");
     ALLOC(c->vis, N, "visible flags");
@@ -631,14 +635,14 @@ static rb_status buildFrom(rb_ctx* c, const rb::Point* ring, const uint32_t* siz
     uint32_t done = 0;
     bool stopped = false;
     if (graphs) {
-        const uint64_t itersBefore = c->hostCtr->expandIters;
+        const uint32_t condBefore = c->hostCtr->condRuns;
         const uint64_t pointsBefore = c->hostCtr->numPointsProcessed;
         for (uint32_t k = 0; k < nb; k++) RB_CUDA(c, cudaGraphLaunch(c->batchGraph, c->stream));
         rb_status st = readCounters(c);
         if (st != RB_OK) return st;
         done = c->hostCtr->batchletIndex - first;
         stopped = c->hostCtr->batchStop && c->hostCtr->stopReason == rb::kStopMemory;
-        countGraphLaunches(c, nb, itersBefore, done, c->hostCtr->numPointsProcessed - pointsBefore);
+        countGraphLaunches(c, nb, condBefore, c->hostCtr->numPointsProcessed - pointsBefore);
         nb = 0;  // the batches ran on the device
     }
     for (uint32_t b = first; b < first + nb; b++) {
@@ -710,7 +714,8 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
     const uint32_t firstBatch = c->batchesConsumed;
     if ((uint64_t)firstBatch + nb > 0xFFFFFFFFull) return fail(c, RB_ERR_CAPACITY, "too many batches");
     const bool graphs = graphPath(c);
-    uint64_t itersBefore = 0, pointsBefore = 0;
+    uint64_t pointsBefore = 0;
+    uint32_t condBefore = 0;
     if (graphs) {
         rb::RingDesc& r = *c->hostRing;
         r.base = reinterpret_cast<unsigned long long>(c->ingestRing);
@@ -724,7 +729,7 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
         r.budgetNs = 0;
         rb_status st = uploadRing(c);
         if (st != RB_OK) return st;
-        itersBefore = c->hostCtr->expandIters;
+        condBefore = c->hostCtr->condRuns;
         pointsBefore = c->hostCtr->numPointsProcessed;
     }
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
@@ -795,7 +800,7 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
         c->batchesConsumed = c->hostCtr->batchletIndex;
         done = c->batchesConsumed - firstBatch;
         stopped = c->hostCtr->batchStop && c->hostCtr->stopReason == rb::kStopMemory;
-        countGraphLaunches(c, nb, itersBefore, done, c->hostCtr->numPointsProcessed - pointsBefore);
+        countGraphLaunches(c, nb, condBefore, c->hostCtr->numPointsProcessed - pointsBefore);
     }
     if (out) {
         float ms = 0.0f;

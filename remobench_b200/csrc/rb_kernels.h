@@ -35,6 +35,7 @@ void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cuda
 void launchRecount(const Dev& d, const Point* pts, uint32_t n, uint32_t prevStamp, int grid, cudaStream_t s);
 void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s);
 void launchZeroGrids(const Dev& d, int grid, cudaStream_t s);
+void launchExpandCond(const Dev& d, cudaStream_t s);
 void launchSpillCopy(const Dev& d, int grid, cudaStream_t s);
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchVoxCommit(const Dev& d, int grid, cudaStream_t s);

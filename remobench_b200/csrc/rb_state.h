@@ -81,7 +81,9 @@ struct Counters {
     uint32_t callBatches;         // batches built since the build call began
     uint32_t accumItems;          // work items of the current Accumulate launch
     uint32_t numZero;             // grids of nodes split this batch, to zero after expand
-    uint32_t pad4;
+    uint32_t histValid;           // hist8 holds the child-octant counts of the nodes to split next
+    uint32_t countLo, countHi;    // nodes [countLo, countHi) whose points the next recount counts
+    uint32_t condRuns;            // runs of the expand loop's test since allocation (wraps)
 };
 
 enum StopReason : uint32_t { kStopMemory = 1u, kStopNoBatch = 2u, kStopTime = 3u };
@@ -214,6 +216,9 @@ struct Dev {
     uint32_t* accumTo;       // [maxNodes]
     uint32_t* accumItem;     // [maxNodes + 1] exclusive prefix of work items
     uint32_t* zeroList;      // [zeroCap] grids to zero after the expand loop
+    // per node, its points per child octant, counted by the recount for the
+    // nodes made by the last split: one level of lookahead for the next split
+    uint32_t* hist8;         // [maxNodes * 8]
     uint32_t zeroCap;
     // capacities and constants
     uint32_t maxNodes;

@@ -113,6 +113,9 @@ __device__ __forceinline__ void blockCountsInit(BlockCounts& b) {
 }
 
 // Every lane of the warp calls it; lanes with nothing to count pass kNone.
+// hist: key is a child-octant bin (node * 8 + octant) of hist8, which takes
+// plain additions; otherwise key is a leaf whose counter is bumped.
+template <bool hist>
 __device__ __forceinline__ void blockCountAt(const Dev& d, BlockCounts& b, uint32_t leaf) {
     const unsigned peers = __match_any_sync(0xFFFFFFFFu, leaf);
     if (leaf == kNone || (int)laneId() != __ffs(peers) - 1) return;
@@ -126,13 +129,19 @@ __device__ __forceinline__ void blockCountAt(const Dev& d, BlockCounts& b, uint3
         }
         slot = (slot + 1u) & (kBlockLeaves - 1u);
     }
-    addCount(d, leaf, g);  // crowded table: count globally
+    // crowded table: count globally
+    if (hist) atomicAdd(&d.hist8[leaf], g);
+    else addCount(d, leaf, g);
 }
 
-// After a barrier: the block's sums into the leaves' counters.
+// After a barrier: the block's sums into the leaves' counters (or hist8).
+template <bool hist>
 __device__ __forceinline__ void blockCountsFlush(const Dev& d, BlockCounts& b) {
-    for (uint32_t t = threadIdx.x; t < kBlockLeaves; t += blockDim.x)
-        if (b.leaf[t] != kNone && b.cnt[t] != 0u) addCount(d, b.leaf[t], b.cnt[t]);
+    for (uint32_t t = threadIdx.x; t < kBlockLeaves; t += blockDim.x) {
+        if (b.leaf[t] == kNone || b.cnt[t] == 0u) continue;
+        if (hist) atomicAdd(&d.hist8[b.leaf[t]], b.cnt[t]);
+        else addCount(d, b.leaf[t], b.cnt[t]);
+    }
 }
 
 // Block-level slot reservation: each item takes the next slot of its key's
@@ -228,6 +237,9 @@ __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     c->iter = 1;
     c->expandGuard = 0;
     c->numZero = 0;
+    c->histValid = 0;
+    c->countLo = 0;
+    c->countHi = 0;
     c->hashNeedsClear = 0;  // k_hash_reset ran before this kernel
 }
 
@@ -239,16 +251,6 @@ __global__ void __launch_bounds__(256) k_hash_reset(Dev d) {
     const ulonglong2 empty = make_ulonglong2(kHashEmpty, kHashEmpty);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x)
         d.hashSlots[i] = empty;
-}
-
-// The expand loop's condition for device-driven builds: another split pass
-// while the last count found spilling nodes. expandGuard bounds the loop even
-// if the counts never settle (max_expand_iters <= 31 passes are needed).
-__global__ void k_expand_cond(Dev d, cudaGraphConditionalHandle h) {
-    Counters* c = d.ctr;
-    const uint32_t g = ++c->expandGuard;
-    const bool more = c->batchStop == 0u && c->numSpill > 0u && g <= 40u;
-    cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 // Iteration 1 of expand (doCounting over the batch, remolod_octree.cu:225-229):
@@ -281,67 +283,72 @@ __global__ void __launch_bounds__(256) k_count_first(Dev d, const Point* __restr
                                    quant20(p.z, d.boxMin[2], d.octreeSize));
             d.leafOf[i] = leaf;
         }
-        blockCountAt(d, s_counts, leaf);
+        blockCountAt<false>(d, s_counts, leaf);
     }
     __syncthreads();
-    blockCountsFlush(d, s_counts);
+    blockCountsFlush<false>(d, s_counts);
 }
 
 // Iterations 2.. of expand. The reference re-descends every batch and spilled
 // point from the root and counts only at leaves created by the last split
 // (countIteration, remolod_octree.cu:203). A point can only reach such a leaf
-// if its own leaf was split, so only those points move, one level, from the
-// leaf they were in; the counts that result are the same.
-__device__ __forceinline__ uint32_t stepIfSplit(const Dev& d, uint32_t cur, const Point& p,
-                                                uint32_t prevStamp) {
-    if (d.splitIter[cur] != prevStamp) return kNone;
-    const uint32_t lv = d.level[cur];
-    if (lv >= (uint32_t)kMaxDepth) return kNone;
-    const uint32_t ci = childIndex(quant20(p.x, d.boxMin[0], d.octreeSize),
-                                   quant20(p.y, d.boxMin[1], d.octreeSize),
-                                   quant20(p.z, d.boxMin[2], d.octreeSize), lv);
-    return (uint32_t)d.child[cur * 8u + ci];
-}
-
-// prevStamp == 0: device-driven; the stamp of the split just made, and no
-// recount once the pass limit is reached (the host loop does not launch it).
+// if its own leaf was split, so only those points move, from the leaf they
+// were in, through the nodes the last split made (one or two levels, see
+// k_split); the counts that result are the same.
+//
+// Points reaching a node in [countLo, countHi) (the deepest nodes the split
+// made) are counted per child octant into hist8: k_expand_cond sums a node's
+// eight bins into its counter and lists the nodes over the limit, and the next
+// split reads the bins to split the spilling nodes' spilling children in the
+// same launch.
+//
+// prevStamp == 0: device-driven; the stamp of the last split's first round,
+// and no recount once the pass limit is reached.
 __global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict__ pts, uint32_t n,
                                                  uint32_t prevStamp) {
-    if (d.ctr->batchStop) return;
+    Counters* c = d.ctr;
+    if (c->batchStop) return;
     if (prevStamp == 0u) {
-        if (d.ctr->iter > d.maxExpandIters) return;
-        prevStamp = d.ctr->lastStamp;
+        if (c->iter > d.maxExpandIters) return;
+        prevStamp = c->lastStamp;
     }
     RB_BATCH_AT_CURSOR(d, pts, n);
     __shared__ BlockCounts s_counts;
     blockCountsInit(s_counts);
     __syncthreads();
-    const uint32_t ns = d.ctr->numSpilled < d.spillCap ? d.ctr->numSpilled : d.spillCap;
+    const uint32_t lo = c->countLo, hi = c->countHi;
+    const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     const uint32_t per = (((total + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
     const uint32_t begin = min(total, blockIdx.x * per), end = min(total, begin + per);
     for (uint32_t base = begin; base < end; base += blockDim.x) {
         const uint32_t i = base + threadIdx.x;
-        uint32_t leaf = kNone;
-        if (i >= end) {
-        } else if (i < n) {
-            const uint32_t cur = d.leafOf[i];
+        uint32_t bin = kNone;
+        if (i < end) {
+            const bool batchPt = i < n;
+            uint32_t cur = batchPt ? d.leafOf[i] : d.spillLeaf[i - n];
             if (d.splitIter[cur] == prevStamp) {
-                leaf = stepIfSplit(d, cur, loadPoint(pts + i), prevStamp);
-                if (leaf != kNone) d.leafOf[i] = leaf;
-            }
-        } else {
-            const uint32_t j = i - n;
-            const uint32_t cur = d.spillLeaf[j];
-            if (d.splitIter[cur] == prevStamp) {
-                leaf = stepIfSplit(d, cur, d.spillPts[j], prevStamp);
-                if (leaf != kNone) d.spillLeaf[j] = leaf;
+                const Point p = batchPt ? loadPoint(pts + i) : d.spillPts[i - n];
+                const uint32_t x = quant20(p.x, d.boxMin[0], d.octreeSize),
+                               y = quant20(p.y, d.boxMin[1], d.octreeSize),
+                               z = quant20(p.z, d.boxMin[2], d.octreeSize);
+                uint32_t lv = d.level[cur];
+                while (lv < (uint32_t)kMaxDepth) {
+                    const int32_t nx = d.child[cur * 8u + childIndex(x, y, z, lv)];
+                    if (nx < 0) break;
+                    cur = (uint32_t)nx;
+                    lv += 1u;
+                }
+                if (batchPt) d.leafOf[i] = cur;
+                else d.spillLeaf[i - n] = cur;
+                if (cur >= lo && cur < hi)
+                    bin = cur * 8u + (lv < (uint32_t)kMaxDepth ? childIndex(x, y, z, lv) : 0u);
             }
         }
-        if (__any_sync(0xFFFFFFFFu, leaf != kNone)) blockCountAt(d, s_counts, leaf);
+        if (__any_sync(0xFFFFFFFFu, bin != kNone)) blockCountAt<true>(d, s_counts, bin);
     }
     __syncthreads();
-    blockCountsFlush(d, s_counts);
+    blockCountsFlush<true>(d, s_counts);
 }
 
 // Block-wide exclusive scan of one value per thread (blockDim.x == 1024).
@@ -369,6 +376,59 @@ __device__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* total, uint32_t* s_
     *total = s_warp[(blockDim.x >> 5) - 1];
     __syncthreads();
     return prefix;
+}
+
+// The expand loop's test, after each count. After a recount it turns the
+// child-octant bins of the nodes in [countLo, countHi) into their counters and
+// lists those over the limit, in increasing id (doCounting's spilling nodes,
+// remolod_octree.cu:213-218); after the first count the crossing list stands.
+// Device-driven builds (h != 0) set the loop's condition: another pass while
+// nodes spill, at most 40 passes (max_expand_iters <= 31 are needed).
+// One block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_expand_cond(Dev d, cudaGraphConditionalHandle h) {
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_run;
+    Counters* c = d.ctr;
+    const uint32_t lo = c->countLo, hi = c->countHi;
+    const bool stop = c->batchStop != 0u;
+    if (threadIdx.x == 0) s_run = 0;
+    __syncthreads();
+    if (!stop && hi > lo) {
+        for (uint32_t f0 = lo; f0 < hi; f0 += blockDim.x) {
+            const uint32_t f = f0 + threadIdx.x;
+            uint32_t spill = 0;
+            if (f < hi) {
+                const uint4* hb = reinterpret_cast<const uint4*>(d.hist8 + (size_t)f * 8u);
+                const uint4 a = hb[0], b = hb[1];
+                const uint32_t cnt = a.x + a.y + a.z + a.w + b.x + b.y + b.z + b.w;
+                d.counter[f] = cnt;
+                spill = cnt > d.maxPointsPerNode ? 1u : 0u;
+            }
+            uint32_t tot;
+            const uint32_t pre = blockExclusiveScan(spill, &tot, s_warp);
+            if (spill && s_run + pre < d.spillingCap) d.spillNodes[s_run + pre] = f;
+            __syncthreads();
+            if (threadIdx.x == 0) s_run += tot;
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (!stop && hi > lo) {
+            uint32_t ns = s_run;
+            if (ns > d.spillingCap) {
+                atomicOr(&c->overflowFlags, (uint32_t)kOvfSpilling);
+                ns = d.spillingCap;
+            }
+            c->numSpill = ns;
+            c->histValid = 1u;  // the listed nodes' bins are their children's counts
+            c->countLo = 0;
+            c->countHi = 0;
+        }
+        c->condRuns++;
+        const uint32_t g = ++c->expandGuard;
+        const bool more = !stop && c->numSpill > 0u && g <= 40u;
+        if (h != 0ull) cudaGraphSetConditional(h, more ? 1u : 0u);
+    }
 }
 
 // Ascending bitonic sort of n ids in place (single block); pads with kNone.
@@ -481,13 +541,15 @@ __device__ __forceinline__ void splitBook(const Dev& d, Counters* c, uint32_t k,
 __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
     __shared__ uint32_t s_sort[kSortSmem];
     __shared__ uint32_t s_warp[32];
-    __shared__ uint32_t s_runPts, s_runChunks, s_acc, s_nn;
+    __shared__ uint32_t s_runPts, s_runChunks, s_acc, s_nn, s_run2;
     __shared__ SplitInfo s_info[kSplitInfo];
     Counters* c = d.ctr;
     if (c->batchStop) return;
     // stamp 0: device-driven, (batch << 5) | pass as the host loop would pass it;
     // read before any thread reaches the barriers below, after which c->iter moves
-    if (stamp == 0u) stamp = (c->batchletIndex << 5) | c->iter;
+    const uint32_t it0 = c->iter;
+    if (stamp == 0u) stamp = (c->batchletIndex << 5) | it0;
+    const bool histValid = c->histValid != 0u;
     uint32_t ns = c->numSpill;
     if (ns > d.spillingCap) ns = d.spillingCap;
     if (ns == 0) {
@@ -596,7 +658,11 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
         const uint32_t lv = info.lv + 1u;
 #pragma unroll
         for (int q = 0; q < 8; q++) d.child[ch * 8u + q] = -1;
-        d.counter[ch] = 0;
+        // the last recount binned the node's points by child octant: the
+        // child's count is known already
+        d.counter[ch] = histValid ? d.hist8[node * 8u + i] : 0u;
+        reinterpret_cast<uint4*>(d.hist8 + (size_t)ch * 8u)[0] = make_uint4(0, 0, 0, 0);
+        reinterpret_cast<uint4*>(d.hist8 + (size_t)ch * 8u)[1] = make_uint4(0, 0, 0, 0);
         d.numPoints[ch] = 0;
         d.level[ch] = lv;
         d.nodeX[ch] = 2u * info.X + ((i >> 2) & 1u);
@@ -623,8 +689,111 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
         crow[lv - 1u] = make_uint2(node, info.grid);
         d.child[node * 8u + i] = (int32_t)ch;
     }
+    // Round two: with the octant counts known, the children over the limit are
+    // split now, as the next pass would (in increasing id, the next 8 ids each),
+    // if that pass would run (a recount follows this split: it0 < pass limit).
+    // Their children's counts are unknown: the next recount counts them.
+    __syncthreads();
+    const uint32_t nn2 = nn + 8u * acc;
+    uint32_t acc2 = 0;
+    bool round2 = false;
+    if (histValid && acc > 0u && it0 < d.maxExpandIters) {
+        round2 = true;
+        const uint32_t room2 = d.maxNodes > nn2 ? (d.maxNodes - nn2) / 8u : 0u;
+        const uint32_t stamp2 = (c->batchletIndex << 5) | (it0 + 1u);
+        if (threadIdx.x == 0) s_run2 = 0;
+        __syncthreads();
+        for (uint32_t t0 = 0; t0 < 8u * acc; t0 += blockDim.x) {
+            const uint32_t t = t0 + threadIdx.x;
+            const uint32_t f = (t < 8u * acc && d.counter[nn + t] > d.maxPointsPerNode) ? 1u : 0u;
+            uint32_t tot;
+            const uint32_t pre = blockExclusiveScan(f, &tot, s_warp);
+            const uint32_t j = s_run2 + pre;
+            if (f && j < room2) {
+                const uint32_t node = nn + t;
+                uint32_t g = arenaAlloc(d, kGridUnits);
+                d.grid[node] = g;
+                atomicAdd(&c->numGrids, 1u);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
+                          (unsigned long long)refAllocSize(kGridBytes));
+                d.splitIter[node] = stamp2;
+                if (g != kNone) {
+                    const uint32_t zi = atomicAdd(&c->numZero, 1u);
+                    if (zi < d.zeroCap) d.zeroList[zi] = g;
+                }
+                d.dirtyStamp[node] = c->buildStamp;
+                const uint32_t di = atomicAdd(&c->numDirty, 1u);
+                if (di < d.maxNodes) d.dirtyList[di] = node;
+                if (j < d.spillingCap) d.spillNodes[j] = node;
+                if (j < kSplitInfo) {
+                    SplitInfo info;
+                    info.node = node;
+                    info.lv = d.level[node];
+                    info.X = d.nodeX[node];
+                    info.Y = d.nodeY[node];
+                    info.Z = d.nodeZ[node];
+                    info.grid = g;
+                    s_info[j] = info;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_run2 += tot;
+            __syncthreads();
+        }
+        const uint32_t want = s_run2;
+        acc2 = want < room2 ? want : room2;
+        if (acc2 > d.spillingCap) acc2 = d.spillingCap;
+        if (threadIdx.x == 0 && acc2 < want) c->nodePoolOverflow = 1;
+        for (uint32_t t = threadIdx.x; t < 8u * acc2; t += blockDim.x) {
+            const uint32_t k = t >> 3, i = t & 7u;
+            SplitInfo info;
+            if (k < kSplitInfo) {
+                info = s_info[k];
+            } else {
+                info.node = d.spillNodes[k];
+                info.grid = d.grid[info.node];
+                info.lv = d.level[info.node];
+                info.X = d.nodeX[info.node];
+                info.Y = d.nodeY[info.node];
+                info.Z = d.nodeZ[info.node];
+            }
+            const uint32_t node = info.node;
+            const uint32_t ch = nn2 + t;
+            const uint32_t lv = info.lv + 1u;
+#pragma unroll
+            for (int q = 0; q < 8; q++) d.child[ch * 8u + q] = -1;
+            d.counter[ch] = 0;
+            reinterpret_cast<uint4*>(d.hist8 + (size_t)ch * 8u)[0] = make_uint4(0, 0, 0, 0);
+            reinterpret_cast<uint4*>(d.hist8 + (size_t)ch * 8u)[1] = make_uint4(0, 0, 0, 0);
+            d.numPoints[ch] = 0;
+            d.level[ch] = lv;
+            d.nodeX[ch] = 2u * info.X + ((i >> 2) & 1u);
+            d.nodeY[ch] = 2u * info.Y + ((i >> 1) & 1u);
+            d.nodeZ[ch] = 2u * info.Z + (i & 1u);
+            d.grid[ch] = kNone;
+            d.numVoxels[ch] = 0;
+            d.numVoxelsStored[ch] = 0;
+            d.numPointChunks[ch] = 0;
+            d.numVoxelChunks[ch] = 0;
+            d.ptTableOff[ch] = kNone;
+            d.ptTableCap[ch] = 0;
+            d.vxTableOff[ch] = kNone;
+            d.vxTableCap[ch] = 0;
+            d.splitIter[ch] = 0;
+            d.dirtyStamp[ch] = 0;
+            AccumI z = {};
+            d.accum[ch] = z;
+            const uint2* prow = d.anc + (size_t)node * kMaxDepth;
+            uint2* crow = d.anc + (size_t)ch * kMaxDepth;
+#pragma unroll
+            for (uint32_t l = 0; l < (uint32_t)kMaxDepth; l++)
+                if (l + 1u < lv) crow[l] = prow[l];
+            crow[lv - 1u] = make_uint2(node, info.grid);
+            d.child[node * 8u + i] = (int32_t)ch;
+        }
+    }
     if (threadIdx.x == 0) {
-        c->numNodes = nn + 8u * acc;
+        c->numNodes = nn2 + 8u * acc2;
         c->numSplit = acc;
         c->spillChunkTotal = s_runChunks;
         uint32_t total = spilledBefore + s_runPts;
@@ -633,10 +802,22 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
             total = d.spillCap;
         }
         c->numSpilled = total;
-        c->nodesSplit += acc;
+        c->nodesSplit += acc + acc2;
         c->numSpill = 0;
         c->lastStamp = stamp;
-        c->iter += 1;
+        c->iter = it0 + (round2 ? 2u : 1u);
+        // the nodes whose points the next recount counts
+        if (!histValid) {
+            c->countLo = nn;
+            c->countHi = nn2;
+        } else if (acc2 > 0u) {
+            c->countLo = nn2;
+            c->countHi = nn2 + 8u * acc2;
+        } else {
+            c->countLo = 0;
+            c->countHi = 0;
+        }
+        c->histValid = 0;
     }
 }
 
@@ -1242,6 +1423,7 @@ void launchRecount(const Dev& d, const Point* pts, uint32_t n, uint32_t prevStam
     k_recount<<<grid, 256, 0, s>>>(d, pts, n, prevStamp);
 }
 void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s) { k_split<<<1, 1024, 0, s>>>(d, stamp); }
+void launchExpandCond(const Dev& d, cudaStream_t s) { k_expand_cond<<<1, 1024, 0, s>>>(d, 0ull); }
 void launchSpillCopy(const Dev& d, int grid, cudaStream_t s) { k_spill_copy<<<grid, 256, 0, s>>>(d); }
 void launchZeroGrids(const Dev& d, int grid, cudaStream_t s) { k_zero_grids<<<grid, 256, 0, s>>>(d); }
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
@@ -1286,7 +1468,7 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &ndeps)) != cudaSuccess) break;
         cudaGraphConditionalHandle h;
         if ((e = cudaGraphConditionalHandleCreate(&h, g, 0u, 0u)) != cudaSuccess) break;
-        k_expand_cond<<<1, 1, 0, cs>>>(d, h);
+        k_expand_cond<<<1, 1024, 0, cs>>>(d, h);
         if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &ndeps)) != cudaSuccess) break;
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
         cp.conditional.handle = h;
@@ -1304,7 +1486,7 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         k_split<<<1, 1024, 0, bs>>>(d, 0u);
         k_spill_copy<<<fixedGrid, 256, 0, bs>>>(d);
         k_recount<<<pointGrid, 256, 0, bs>>>(d, nullptr, 0u, 0u);
-        k_expand_cond<<<1, 1, 0, bs>>>(d, h);
+        k_expand_cond<<<1, 1024, 0, bs>>>(d, h);
         cudaGraph_t bodyOut = nullptr;
         if ((e = cudaStreamEndCapture(bs, &bodyOut)) != cudaSuccess) break;
         k_zero_grids<<<fixedGrid, 256, 0, cs>>>(d);

@@ -922,6 +922,12 @@ __device__ __forceinline__ uint32_t cellAt(uint32_t x28, uint32_t y28, uint32_t 
 }
 
 constexpr uint32_t kInsertGroup = 4;  // table updates a lane keeps in flight
+// Per-block cache of cells this block's points lead, direct-mapped: entry
+// (tag << 32) | global point index, tag = key >> kCellCacheBits (under 2^31,
+// since node ids stay below 2^21), position = the key's low bits plus a hash of
+// the tag, so tag and position give back the key.
+constexpr uint32_t kCellCacheBits = 11;
+constexpr uint32_t kCellCache = 1u << kCellCacheBits;
 // Per-warp buffer of claimed table slots: under 32 waiting plus one group of
 // at most 32 lanes x kInsertGroup claims.
 constexpr uint32_t kWarpCells = 32u + 32u * kInsertGroup;
@@ -953,11 +959,19 @@ __device__ __forceinline__ void flushWarpCells(const Dev& d, const uint32_t* wbu
 // lowest index; spilled points use a full match); (3) each lane's table
 // updates in groups: all slot reads, then all claims, then all minimum
 // updates, with one new-cell counter bump per warp and group. A slot already
-// holding a lower index is left alone.
+// holding a lower index is left alone. Between (2) and (3) a leader whose cell
+// an earlier point of the same block already leads (a lower index, or any
+// point in first-come mode) drops out: that point's update keeps the table's
+// result, and most of a block's leaders repeat cells its other warps lead.
 __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restrict__ pts, uint32_t n) {
     __shared__ uint32_t s_wbuf[256 / 32][kWarpCells];
+    __shared__ unsigned long long s_cells[kCellCache];
     const Counters* c = d.ctr;
     if (c->batchStop) return;
+    for (uint32_t t = threadIdx.x; t < kCellCache; t += blockDim.x) s_cells[t] = ~0ull;
+    __syncthreads();
+    // single 64-bit accesses: an entry is read and written whole
+    volatile unsigned long long* cells = s_cells;
     RB_BATCH_AT_CURSOR(d, pts, n);
     uint32_t* wbuf = s_wbuf[threadIdx.x >> 5];
     uint32_t wbufN = 0;  // the same in every lane of the warp
@@ -1051,6 +1065,13 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
                 const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
                 if (lowest) first = key != kHashEmpty && gidx == __reduce_min_sync(peers, gidx);
                 else first = key != kHashEmpty && lane == (uint32_t)(__ffs(peers) - 1);
+            }
+            if (first) {
+                const uint32_t tag = (uint32_t)(key >> kCellCacheBits);
+                const uint32_t e = ((uint32_t)key + ((tag * 0x9E3779B1u) >> (32u - kCellCacheBits))) & (kCellCache - 1u);
+                const unsigned long long held = cells[e];
+                if ((uint32_t)(held >> 32) == tag && (!lowest || (uint32_t)held < gidx)) first = false;
+                else cells[e] = ((unsigned long long)tag << 32) | gidx;
             }
             if (first) lead |= 1u << l;
         }

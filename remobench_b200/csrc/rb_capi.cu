@@ -27,7 +27,7 @@ enum KernelId : int {
     K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END, K_ACCUMULATE, K_ACCUM_VERIFY,
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
-    K_HASH_RESET, K_EXPAND_COND, K_ZERO_GRIDS, K_NUM
+    K_HASH_RESET, K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_SKIPPED, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
@@ -35,7 +35,9 @@ static const char* const kKernelNames[K_NUM] = {
     "k_accumulate", "k_accum_verify", "k_sweep", "k_reset_root", "k_fb_clear", "k_node_flags",
     "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve", "k_roll_level", "k_analyze",
     "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam", "k_hash_reset",
-    "k_expand_cond", "k_zero_grids"};
+    "k_expand_cond", "k_zero_grids",
+    // the four launches of an unrolled expand pass after the loop ended
+    "k_expand_skipped"};
 
 struct Profiler {
     bool on = false;
@@ -263,16 +265,19 @@ bool graphPath(rb_ctx* c) {
 
 // Launches of one graph batch, for the per-kernel counts: eleven fixed
 // kernels per batch, four per pass of the expand loop.
-void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint64_t points) {
+void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint32_t skipsBefore, uint64_t points) {
     // every batch graph runs the loop test once after its first count and once
-    // after each split pass
+    // after each split pass; an unrolled pass after the loop ended launches its
+    // four kernels, which return at once
     const uint32_t conds = c->hostCtr->condRuns - condBefore;
+    const uint32_t skips = c->hostCtr->condSkips - skipsBefore;
     const uint64_t passes = conds >= batches ? conds - batches : 0u;
     for (int k : {K_HASH_RESET, K_BATCH_BEGIN, K_COUNT_FIRST, K_ZERO_GRIDS, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS,
                   K_INSERT, K_VOX_STORE, K_BATCH_END})
         c->prof.launches[k] += batches;
     c->prof.launches[K_EXPAND_COND] += conds;
     for (int k : {K_SPLIT, K_SPILL_COPY, K_RECOUNT}) c->prof.launches[k] += passes;
+    c->prof.launches[K_EXPAND_SKIPPED] += 4ull * skips;
     for (int k : {K_COUNT_FIRST, K_VOX_SAMPLE, K_INSERT}) c->prof.units[k] += points;
 }
 
@@ -635,14 +640,14 @@ static rb_status buildFrom(rb_ctx* c, const rb::Point* ring, const uint32_t* siz
     uint32_t done = 0;
     bool stopped = false;
     if (graphs) {
-        const uint32_t condBefore = c->hostCtr->condRuns;
+        const uint32_t condBefore = c->hostCtr->condRuns, skipsBefore = c->hostCtr->condSkips;
         const uint64_t pointsBefore = c->hostCtr->numPointsProcessed;
         for (uint32_t k = 0; k < nb; k++) RB_CUDA(c, cudaGraphLaunch(c->batchGraph, c->stream));
         rb_status st = readCounters(c);
         if (st != RB_OK) return st;
         done = c->hostCtr->batchletIndex - first;
         stopped = c->hostCtr->batchStop && c->hostCtr->stopReason == rb::kStopMemory;
-        countGraphLaunches(c, nb, condBefore, c->hostCtr->numPointsProcessed - pointsBefore);
+        countGraphLaunches(c, nb, condBefore, skipsBefore, c->hostCtr->numPointsProcessed - pointsBefore);
         nb = 0;  // the batches ran on the device
     }
     for (uint32_t b = first; b < first + nb; b++) {
@@ -715,7 +720,7 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
     if ((uint64_t)firstBatch + nb > 0xFFFFFFFFull) return fail(c, RB_ERR_CAPACITY, "too many batches");
     const bool graphs = graphPath(c);
     uint64_t pointsBefore = 0;
-    uint32_t condBefore = 0;
+    uint32_t condBefore = 0, skipsBefore = 0;
     if (graphs) {
         rb::RingDesc& r = *c->hostRing;
         r.base = reinterpret_cast<unsigned long long>(c->ingestRing);
@@ -730,6 +735,7 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
         rb_status st = uploadRing(c);
         if (st != RB_OK) return st;
         condBefore = c->hostCtr->condRuns;
+        skipsBefore = c->hostCtr->condSkips;
         pointsBefore = c->hostCtr->numPointsProcessed;
     }
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
@@ -800,7 +806,7 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
         c->batchesConsumed = c->hostCtr->batchletIndex;
         done = c->batchesConsumed - firstBatch;
         stopped = c->hostCtr->batchStop && c->hostCtr->stopReason == rb::kStopMemory;
-        countGraphLaunches(c, nb, condBefore, c->hostCtr->numPointsProcessed - pointsBefore);
+        countGraphLaunches(c, nb, condBefore, skipsBefore, c->hostCtr->numPointsProcessed - pointsBefore);
     }
     if (out) {
         float ms = 0.0f;

@@ -56,12 +56,12 @@ struct Counters {
     uint32_t numSpilled;          // spilled points this batch
     uint32_t numNew;              // new voxel cells this batch
     uint32_t spillChunkTotal;     // copy work items of the last split
-    uint32_t pad0;
+    uint32_t loopMore;            // the last loop test's answer: another expand pass
     // flags and diagnostics (sticky until reset)
     uint32_t memCapacityReached;
     uint32_t nodePoolOverflow;
     uint32_t overflowFlags;       // RB_OVF_* bits
-    uint32_t pad1;
+    uint32_t condSkips;           // unrolled expand passes skipped after the loop ended (wraps)
     uint64_t droppedPoints;
     uint64_t expandIters;
     uint64_t nodesSplit;

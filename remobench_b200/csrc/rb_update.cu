@@ -305,9 +305,9 @@ __global__ void __launch_bounds__(256) k_count_first(Dev d, const Point* __restr
 // prevStamp == 0: device-driven; the stamp of the last split's first round,
 // and no recount once the pass limit is reached.
 __global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict__ pts, uint32_t n,
-                                                 uint32_t prevStamp) {
+                                                 uint32_t prevStamp, uint32_t gated) {
     Counters* c = d.ctr;
-    if (c->batchStop) return;
+    if (c->batchStop || (gated && c->loopMore == 0u)) return;
     if (prevStamp == 0u) {
         if (c->iter > d.maxExpandIters) return;
         prevStamp = c->lastStamp;
@@ -385,10 +385,19 @@ __device__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* total, uint32_t* s_
 // Device-driven builds (h != 0) set the loop's condition: another pass while
 // nodes spill, at most 40 passes (max_expand_iters <= 31 are needed).
 // One block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_expand_cond(Dev d, cudaGraphConditionalHandle h) {
+__global__ void __launch_bounds__(1024) k_expand_cond(Dev d, cudaGraphConditionalHandle h, uint32_t gated) {
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_run;
     Counters* c = d.ctr;
+    // a pass after the loop ended: keep it ended (every thread reads the flag
+    // before the barrier after which thread 0 rewrites it)
+    if (gated && c->loopMore == 0u) {
+        if (threadIdx.x == 0) {
+            c->condSkips++;
+            if (h != 0ull) cudaGraphSetConditional(h, 0u);
+        }
+        return;
+    }
     const uint32_t lo = c->countLo, hi = c->countHi;
     const bool stop = c->batchStop != 0u;
     if (threadIdx.x == 0) s_run = 0;
@@ -427,6 +436,7 @@ __global__ void __launch_bounds__(1024) k_expand_cond(Dev d, cudaGraphConditiona
         c->condRuns++;
         const uint32_t g = ++c->expandGuard;
         const bool more = !stop && c->numSpill > 0u && g <= 40u;
+        c->loopMore = more ? 1u : 0u;
         if (h != 0ull) cudaGraphSetConditional(h, more ? 1u : 0u);
     }
 }
@@ -538,13 +548,13 @@ __device__ __forceinline__ void splitBook(const Dev& d, Counters* c, uint32_t k,
 // the reference's 36M cloud, wiki/03_ExpandStageFindings.md:63) are sorted,
 // scanned and booked by one warp with no block barrier; more go through a
 // block-wide sort and scans.
-__global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
+__global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp, uint32_t gated) {
     __shared__ uint32_t s_sort[kSortSmem];
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_runPts, s_runChunks, s_acc, s_nn, s_run2;
     __shared__ SplitInfo s_info[kSplitInfo];
     Counters* c = d.ctr;
-    if (c->batchStop) return;
+    if (c->batchStop || (gated && c->loopMore == 0u)) return;
     // stamp 0: device-driven, (batch << 5) | pass as the host loop would pass it;
     // read before any thread reaches the barriers below, after which c->iter moves
     const uint32_t it0 = c->iter;
@@ -824,9 +834,9 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp) {
 // The split nodes' stored points move to the spill list (remolod_octree.cu:250-285)
 // and their chunks return to the queue (:349-360): one work item per owned
 // chunk, strided over blocks.
-__global__ void __launch_bounds__(256) k_spill_copy(Dev d) {
+__global__ void __launch_bounds__(256) k_spill_copy(Dev d, uint32_t gated) {
     const Counters* c = d.ctr;
-    if (c->batchStop) return;
+    if (c->batchStop || (gated && c->loopMore == 0u)) return;
     const uint32_t nsplit = c->numSplit;
     const uint32_t nchunk = c->spillChunkTotal;
     for (uint32_t w = blockIdx.x; w < nchunk; w += gridDim.x) {
@@ -1441,11 +1451,11 @@ void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cuda
 }
 void launchRecount(const Dev& d, const Point* pts, uint32_t n, uint32_t prevStamp, int grid,
                    cudaStream_t s) {
-    k_recount<<<grid, 256, 0, s>>>(d, pts, n, prevStamp);
+    k_recount<<<grid, 256, 0, s>>>(d, pts, n, prevStamp, 0u);
 }
-void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s) { k_split<<<1, 1024, 0, s>>>(d, stamp); }
-void launchExpandCond(const Dev& d, cudaStream_t s) { k_expand_cond<<<1, 1024, 0, s>>>(d, 0ull); }
-void launchSpillCopy(const Dev& d, int grid, cudaStream_t s) { k_spill_copy<<<grid, 256, 0, s>>>(d); }
+void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s) { k_split<<<1, 1024, 0, s>>>(d, stamp, 0u); }
+void launchExpandCond(const Dev& d, cudaStream_t s) { k_expand_cond<<<1, 1024, 0, s>>>(d, 0ull, 0u); }
+void launchSpillCopy(const Dev& d, int grid, cudaStream_t s) { k_spill_copy<<<grid, 256, 0, s>>>(d, 0u); }
 void launchZeroGrids(const Dev& d, int grid, cudaStream_t s) { k_zero_grids<<<grid, 256, 0, s>>>(d); }
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_vox_sample<<<grid, 256, 0, s>>>(d, pts, n);
@@ -1465,6 +1475,12 @@ void launchResetRoot(const Dev& d, int grid, cudaStream_t s) { k_reset_root<<<gr
 // device cursor. One graph launch builds the batch at batchletIndex with no
 // host round trip; a stopped batch (memory, no batch uploaded, time budget)
 // runs through as no-ops.
+// Expand passes captured as plain kernels ahead of the loop node: a pass after
+// the loop ended costs four launches that return at once, while entering and
+// leaving a conditional node's body costs several microseconds per pass and
+// per batch. Batches that need more passes finish in the loop node.
+constexpr int kUnrolledPasses = 4;
+
 cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGraphExec_t* out) {
     *out = nullptr;
     cudaStream_t cs = nullptr, bs = nullptr;
@@ -1489,7 +1505,13 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &ndeps)) != cudaSuccess) break;
         cudaGraphConditionalHandle h;
         if ((e = cudaGraphConditionalHandleCreate(&h, g, 0u, 0u)) != cudaSuccess) break;
-        k_expand_cond<<<1, 1024, 0, cs>>>(d, h);
+        k_expand_cond<<<1, 1024, 0, cs>>>(d, h, 0u);
+        for (int pass = 0; pass < kUnrolledPasses; pass++) {
+            k_split<<<1, 1024, 0, cs>>>(d, 0u, 1u);
+            k_spill_copy<<<fixedGrid, 256, 0, cs>>>(d, 1u);
+            k_recount<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u, 0u, 1u);
+            k_expand_cond<<<1, 1024, 0, cs>>>(d, h, 1u);
+        }
         if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &ndeps)) != cudaSuccess) break;
         cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
         cp.conditional.handle = h;
@@ -1504,10 +1526,10 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         if ((e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
             cudaSuccess)
             break;
-        k_split<<<1, 1024, 0, bs>>>(d, 0u);
-        k_spill_copy<<<fixedGrid, 256, 0, bs>>>(d);
-        k_recount<<<pointGrid, 256, 0, bs>>>(d, nullptr, 0u, 0u);
-        k_expand_cond<<<1, 1024, 0, bs>>>(d, h);
+        k_split<<<1, 1024, 0, bs>>>(d, 0u, 0u);
+        k_spill_copy<<<fixedGrid, 256, 0, bs>>>(d, 0u);
+        k_recount<<<pointGrid, 256, 0, bs>>>(d, nullptr, 0u, 0u, 0u);
+        k_expand_cond<<<1, 1024, 0, bs>>>(d, h, 0u);
         cudaGraph_t bodyOut = nullptr;
         if ((e = cudaStreamEndCapture(bs, &bodyOut)) != cudaSuccess) break;
         k_zero_grids<<<fixedGrid, 256, 0, cs>>>(d);

@@ -331,7 +331,7 @@ def main():
                       "k_recount": 4.0, "k_accumulate": 16.0}
     # DRAM bytes (read + write) per launch from one ncu capture of the kernel on
     # 1M-point batches of the same generator (profiles/k_vox_sample_config2_1M_batch.md)
-    ncu_traffic = {"k_vox_sample": 43.3e6}
+    ncu_traffic = {"k_vox_sample": 43.1e6}
     peak, peak_kind = peaks()
     roof = None
     if top[0] in bytes_per_unit and top[1]["units"] > 0:

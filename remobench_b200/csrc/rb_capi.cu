@@ -27,14 +27,14 @@ enum KernelId : int {
     K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END, K_ACCUMULATE, K_ACCUM_VERIFY,
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
-    K_HASH_RESET, K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_SKIPPED, K_NUM
+    K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_SKIPPED, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
     "k_vox_sample", "k_vox_commit", "k_alloc_chunks", "k_insert", "k_vox_store", "k_batch_end",
     "k_accumulate", "k_accum_verify", "k_sweep", "k_reset_root", "k_fb_clear", "k_node_flags",
     "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve", "k_roll_level", "k_analyze",
-    "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam", "k_hash_reset",
+    "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam",
     "k_expand_cond", "k_zero_grids",
     // the four launches of an unrolled expand pass after the loop ended
     "k_expand_skipped"};
@@ -219,7 +219,6 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
     const Dev& d = c->d;
     cudaStream_t s = c->stream;
     *stopped = false;
-    LAUNCH(c, K_HASH_RESET, 0, rb::launchHashReset(d, c->numSMs * 8, s));
     LAUNCH(c, K_BATCH_BEGIN, 1, rb::launchBatchBegin(d, s));
     LAUNCH(c, K_COUNT_FIRST, n, rb::launchCountFirst(d, pts, n, pointGrid(c, n), s));
     const int fixedGrid = c->numSMs * 4;
@@ -272,7 +271,7 @@ void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint32
     const uint32_t conds = c->hostCtr->condRuns - condBefore;
     const uint32_t skips = c->hostCtr->condSkips - skipsBefore;
     const uint64_t passes = conds >= batches ? conds - batches : 0u;
-    for (int k : {K_HASH_RESET, K_BATCH_BEGIN, K_COUNT_FIRST, K_ZERO_GRIDS, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS,
+    for (int k : {K_BATCH_BEGIN, K_COUNT_FIRST, K_ZERO_GRIDS, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS,
                   K_INSERT, K_VOX_STORE, K_BATCH_END})
         c->prof.launches[k] += batches;
     c->prof.launches[K_EXPAND_COND] += conds;

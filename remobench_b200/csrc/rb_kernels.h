@@ -28,7 +28,6 @@ struct RenderScratch {
 
 // Update
 void launchBatchBegin(const Dev& d, cudaStream_t s);
-void launchHashReset(const Dev& d, int grid, cudaStream_t s);
 // One batch at the device cursor as an instantiated graph (see rb_update.cu).
 cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGraphExec_t* out);
 void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);

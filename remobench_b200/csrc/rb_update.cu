@@ -240,17 +240,7 @@ __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     c->histValid = 0;
     c->countLo = 0;
     c->countHi = 0;
-    c->hashNeedsClear = 0;  // k_hash_reset ran before this kernel
-}
-
-// Empties the whole cell table after a batch overflowed it (its list of new
-// cells could not name every entry, so k_vox_store could not clear them).
-__global__ void __launch_bounds__(256) k_hash_reset(Dev d) {
-    if (d.ctr->hashNeedsClear == 0u) return;
-    const uint32_t size = d.hashMask + 1u;
-    const ulonglong2 empty = make_ulonglong2(kHashEmpty, kHashEmpty);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x)
-        d.hashSlots[i] = empty;
+    c->hashNeedsClear = 0;  // the last batch's k_vox_store emptied the table
 }
 
 // Iteration 1 of expand (doCounting over the batch, remolod_octree.cu:225-229):
@@ -1362,6 +1352,14 @@ __global__ void __launch_bounds__(256) k_vox_store(Dev d) {
             if (phys != kNone) chunkPoints(d, phys)[s % ppc] = v;
         }
     }
+    // new cells beyond the list's capacity left entries that k_vox_commit
+    // could not name: empty the whole table for the next batch
+    if (c->hashNeedsClear) {
+        const uint32_t size = d.hashMask + 1u;
+        const ulonglong2 empty = make_ulonglong2(kHashEmpty, kHashEmpty);
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < size; i += gridDim.x * blockDim.x)
+            d.hashSlots[i] = empty;
+    }
 }
 
 // n == kNone: the batch at the device cursor.
@@ -1409,7 +1407,6 @@ __global__ void k_reset_root(Dev d) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         Counters z = {};
         z.buildStamp = c->buildStamp;
-        z.hashNeedsClear = c->hashNeedsClear;  // stale table entries outlive a reset
         *c = z;
         c->refOffset = 16;
         c->numNodes = 1;
@@ -1445,7 +1442,6 @@ __global__ void k_reset_root(Dev d) {
 // ------------------------------------------------------------------ launches
 
 void launchBatchBegin(const Dev& d, cudaStream_t s) { k_batch_begin<<<1, 1, 0, s>>>(d, 0u); }
-void launchHashReset(const Dev& d, int grid, cudaStream_t s) { k_hash_reset<<<grid, 256, 0, s>>>(d); }
 void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_count_first<<<grid, 256, 0, s>>>(d, pts, n);
 }
@@ -1495,7 +1491,6 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
     do {
         if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) break;
         capturing = true;
-        k_hash_reset<<<pointGrid, 256, 0, cs>>>(d);
         k_batch_begin<<<1, 1, 0, cs>>>(d, 1u);
         k_count_first<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         cudaStreamCaptureStatus status;

@@ -85,7 +85,13 @@ typedef struct rb_config {
     uint32_t drawlist_capacity;      /* 131072 */
     uint64_t safety_margin;          /* 200,000,000 bytes */
     uint32_t use_graphs;             /* 1: each batch is one CUDA graph launch, expand loop on the device; 0: host-driven loop */
-    uint32_t reserved[7];
+    uint32_t backlog_capacity;       /* new voxel cells one batch can list (remolod_octree.cu:26 holds 10,000,000);
+                                        0 = 2 x slot_capacity rounded up to a power of two. The cell table has
+                                        twice as many 16-byte slots, so 10,000,000 takes 512 MB and misses L2
+                                        more often than the default's 64 MB at 1M-point slots. A batch with more
+                                        new cells keeps the first ones and sets RB_OVF_BACKLOG, as the reference
+                                        does at its limit. */
+    uint32_t reserved[6];
 } rb_config;
 
 /* CloudMeta (include/remo/PointSource.h:16-32), headless subset. */

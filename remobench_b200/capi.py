@@ -29,7 +29,8 @@ class Config(ctypes.Structure):
                 ("ring_slots", u32), ("slot_capacity", u32), ("max_batches_per_build", u32),
                 ("time_budget_ms", f32), ("voxel_mode", u32), ("accumulate", u32),
                 ("spilled_capacity", u32), ("spilling_nodes_capacity", u32), ("drawlist_capacity", u32),
-                ("safety_margin", u64), ("use_graphs", u32), ("reserved", u32 * 7)]
+                ("safety_margin", u64), ("use_graphs", u32), ("backlog_capacity", u32),
+                ("reserved", u32 * 6)]
 
 
 class CloudMeta(ctypes.Structure):

@@ -347,7 +347,7 @@ rb_status rb_create(const rb_config* cfg, rb_ctx** out) {
     if (cfg->pipeline > RB_PIPELINE_FLAT || cfg->max_nodes < 9 || cfg->points_per_chunk == 0 ||
         cfg->slot_capacity == 0 || cfg->ring_slots == 0 || cfg->max_expand_iters == 0 ||
         cfg->max_expand_iters > 31 || cfg->voxel_mode > RB_VOXEL_FIRST_COME ||
-        cfg->max_nodes > (1u << 21))
+        cfg->max_nodes > (1u << 21) || cfg->backlog_capacity > (1u << 28))
         return RB_ERR_INVALID_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -496,9 +496,11 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     d.tablePoolCap = (uint32_t)std::min<uint64_t>(128ull * cfg.max_nodes + 4ull * maxChunks, 1ull << 31);
     d.spillCap = cfg.spilled_capacity;
     d.spillingCap = cfg.spilling_nodes_capacity;
-    const uint32_t hashSize = nextPow2(4ull * cfg.slot_capacity);
+    // the cell table keeps its load at or under one half
+    const uint32_t hashSize = cfg.backlog_capacity ? nextPow2(2ull * cfg.backlog_capacity)
+                                                   : nextPow2(4ull * cfg.slot_capacity);
     d.hashMask = hashSize - 1;
-    d.newCap = hashSize / 2;
+    d.newCap = cfg.backlog_capacity ? cfg.backlog_capacity : hashSize / 2;
 
     const uint32_t N = cfg.max_nodes;
     rb_status st = RB_OK;

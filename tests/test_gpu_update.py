@@ -113,3 +113,30 @@ def test_device_time_budget_paces_but_keeps_the_tree(c1_cloud, c1_pair):
     assert calls == 8
     assert np.array_equal(paced.nodes(), ctx.nodes())
     compare_accums(paced, tree)
+
+
+def test_backlog_overflow_leaves_no_stale_cells(c1_cloud):
+    """A batch with more new cells than the backlog holds lists the first
+    backlog_capacity of them and flags RB_OVF_BACKLOG, as the reference does at
+    its limit. The cell table is empty again before the next batch: a second
+    batch of the same points (which splits nodes and makes new cells of its
+    own) claims every cell the first one lost, so the occupancy grids and voxel
+    count end equal to the oracle's, whose 10M backlog never fills here. A cell
+    left behind in the table would stay unclaimed and its bit clear."""
+    cfg, cloud, bmin, bmax = c1_cloud
+    first = cloud[: cfg.batch_size]
+    twice = np.concatenate([first, first])
+    first_cells = build_oracle(first, bmin, bmax, cfg.batch_size).stats().num_voxels
+    tree = build_oracle(twice, bmin, bmax, cfg.batch_size)
+    total_cells = tree.stats().num_voxels
+    # the first batch overflows; the second batch's new cells (its own plus the
+    # ones the first lost: total - cap) fit
+    half = (total_cells + 1) // 2
+    assert half < first_cells
+    cap = (half + first_cells) // 2
+    ctx, _ = build_gpu(twice, bmin, bmax, cfg.batch_size, backlog_capacity=cap)
+    s, o = ctx.stats(), tree.stats()
+    assert s.overflow_flags & 2  # RB_OVF_BACKLOG
+    assert o.overflow_flags == 0
+    assert (s.num_nodes, s.num_points, s.num_voxels) == (o.num_nodes, o.num_points, o.num_voxels)
+    compare_grids(ctx, tree, ctx.nodes())

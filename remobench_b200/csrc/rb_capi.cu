@@ -241,7 +241,8 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
     const uint64_t work = n;
     LAUNCH(c, K_ZERO_GRIDS, 0, rb::launchZeroGrids(d, fixedGrid, s));
     LAUNCH(c, K_VOX_SAMPLE, n, rb::launchVoxSample(d, pts, n, pointGrid(c, work), s));
-    LAUNCH(c, K_VOX_COMMIT, 0, rb::launchVoxCommit(d, c->numSMs * 8, s));
+    // four blocks per SM: fewer blocks, fewer reservations on a node's voxel counter
+    LAUNCH(c, K_VOX_COMMIT, 0, rb::launchVoxCommit(d, fixedGrid, s));
     LAUNCH(c, K_ALLOC_CHUNKS, 0, rb::launchAllocChunks(d, fixedGrid, s));
     LAUNCH(c, K_INSERT, n, rb::launchInsert(d, pts, n, pointGrid(c, work), s));
     LAUNCH(c, K_VOX_STORE, 0, rb::launchVoxStore(d, fixedGrid, s));

@@ -1151,8 +1151,58 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
     flushWarpCells(d, wbuf, wbufN);
 }
 
+// blockReserve for kCommitPerThread keys per thread at once: every key's
+// count merges into the block table first, then one barrier pair hands out
+// the global reservations. Every thread of the block calls it.
+constexpr uint32_t kCommitPerThread = 4;
+
+__device__ __forceinline__ void blockReserveMany(BlockSlots& b, uint32_t* counters,
+                                                 const uint32_t (&key)[kCommitPerThread],
+                                                 uint32_t (&out)[kCommitPerThread]) {
+    const uint32_t lane = laneId();
+    uint32_t at[kCommitPerThread], off[kCommitPerThread], rank[kCommitPerThread];
+#pragma unroll
+    for (uint32_t j = 0; j < kCommitPerThread; j++) {
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, key[j]);
+        const int leader = __ffs(peers) - 1;
+        rank[j] = __popc(peers & ((1u << lane) - 1u));
+        uint32_t s = kNone, o = 0;
+        if (key[j] != kNone && (int)lane == leader) {
+            const uint32_t g = __popc(peers);
+            uint32_t h = (key[j] * 0x9E3779B1u) >> 26;
+            for (uint32_t probe = 0; probe < 8u; probe++) {
+                const uint32_t cur = atomicCAS(&b.key[h], kNone, key[j]);
+                if (cur == kNone || cur == key[j]) {
+                    s = h;
+                    o = atomicAdd(&b.cnt[h], g);
+                    break;
+                }
+                h = (h + 1u) & (kBlockLeaves - 1u);
+            }
+            if (s == kNone) o = atomicAdd(&counters[key[j]], g);  // crowded table: reserve globally
+        }
+        at[j] = __shfl_sync(0xFFFFFFFFu, s, leader);
+        off[j] = __shfl_sync(0xFFFFFFFFu, o, leader);
+    }
+    __syncthreads();
+    // one global reservation per key; the table empties for the next call
+    // (which writes base only after its own first barrier)
+    for (uint32_t t = threadIdx.x; t < kBlockLeaves; t += blockDim.x) {
+        if (b.key[t] != kNone) b.base[t] = atomicAdd(&counters[b.key[t]], b.cnt[t]);
+        b.key[t] = kNone;
+        b.cnt[t] = 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t j = 0; j < kCommitPerThread; j++)
+        out[j] = key[j] == kNone ? kNone : (at[j] != kNone ? b.base[at[j]] : 0u) + off[j] + rank[j];
+}
+
 // Sets the new cells' bits and gives each new voxel its slot in its node
 // (sampleVoxel :119-138). Keys are unique, so every bit is set exactly once.
+// A thread takes kCommitPerThread list entries (a block's entries in steps of
+// blockDim.x) and issues each step's loads for all of them before using any,
+// so one iteration waits on three rounds of memory instead of three per entry.
 __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
     __shared__ BlockSlots s_slots;
     const Counters* c = d.ctr;
@@ -1162,23 +1212,43 @@ __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
     const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
     const uint32_t per = (((nnew + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
     const uint32_t begin = min(nnew, blockIdx.x * per), end = min(nnew, begin + per);
-    for (uint32_t base = begin; base < end; base += blockDim.x) {
-        const uint32_t e = base + threadIdx.x;
-        uint32_t node = kNone;
-        if (e < end) {
-            // the table is final here: move the cell out of it and free the slot
-            const uint32_t slot = d.hashNew[e];
-            const ulonglong2 kv = d.hashSlots[slot];
-            d.hashSlots[slot] = make_ulonglong2(kHashEmpty, kHashEmpty);
-            node = (uint32_t)(kv.x >> 21);
-            const uint32_t vi = (uint32_t)(kv.x & 0x1FFFFFull);
-            atomicOr(gridWordsAt(d, d.grid[node]) + (vi >> 5), 1u << (vi & 31u));
-            d.hashNewNode[e] = node;
-            d.hashNewCell[e] = vi;
-            d.hashNewColor[e] = (uint32_t)(kv.y & 0xFFFFFFFFull);
+    for (uint32_t base = begin; base < end; base += blockDim.x * kCommitPerThread) {
+        uint32_t e[kCommitPerThread], slot[kCommitPerThread], node[kCommitPerThread];
+        ulonglong2 kv[kCommitPerThread];
+#pragma unroll
+        for (uint32_t j = 0; j < kCommitPerThread; j++) {
+            e[j] = base + j * blockDim.x + threadIdx.x;
+            slot[j] = e[j] < end ? d.hashNew[e[j]] : kNone;
         }
-        const uint32_t s = blockReserve(s_slots, d.numVoxels, node);
-        if (node != kNone) d.hashNewSlot[e] = s;
+#pragma unroll
+        for (uint32_t j = 0; j < kCommitPerThread; j++)
+            kv[j] = slot[j] != kNone ? d.hashSlots[slot[j]] : make_ulonglong2(kHashEmpty, 0ull);
+        uint32_t g[kCommitPerThread];
+#pragma unroll
+        for (uint32_t j = 0; j < kCommitPerThread; j++) {
+            node[j] = kNone;
+            g[j] = 0;
+            if (slot[j] != kNone) {
+                // the table is final here: move the cell out of it and free the slot
+                d.hashSlots[slot[j]] = make_ulonglong2(kHashEmpty, kHashEmpty);
+                node[j] = (uint32_t)(kv[j].x >> 21);
+                g[j] = d.grid[node[j]];
+            }
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kCommitPerThread; j++) {
+            if (node[j] == kNone) continue;
+            const uint32_t vi = (uint32_t)(kv[j].x & 0x1FFFFFull);
+            atomicOr(gridWordsAt(d, g[j]) + (vi >> 5), 1u << (vi & 31u));
+            d.hashNewNode[e[j]] = node[j];
+            d.hashNewCell[e[j]] = vi;
+            d.hashNewColor[e[j]] = (uint32_t)(kv[j].y & 0xFFFFFFFFull);
+        }
+        uint32_t s[kCommitPerThread];
+        blockReserveMany(s_slots, d.numVoxels, node, s);
+#pragma unroll
+        for (uint32_t j = 0; j < kCommitPerThread; j++)
+            if (node[j] != kNone) d.hashNewSlot[e[j]] = s[j];
     }
 }
 
@@ -1529,7 +1599,7 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         if ((e = cudaStreamEndCapture(bs, &bodyOut)) != cudaSuccess) break;
         k_zero_grids<<<fixedGrid, 256, 0, cs>>>(d);
         k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
-        k_vox_commit<<<pointGrid, 256, 0, cs>>>(d);
+        k_vox_commit<<<fixedGrid, 256, 0, cs>>>(d);
         k_alloc_chunks<<<fixedGrid, 256, 0, cs>>>(d);
         k_insert<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         k_vox_store<<<fixedGrid, 256, 0, cs>>>(d);

@@ -1151,18 +1151,20 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
     flushWarpCells(d, wbuf, wbufN);
 }
 
-// blockReserve for kCommitPerThread keys per thread at once: every key's
+// blockReserve for kEntriesPerThread keys per thread at once: every key's
 // count merges into the block table first, then one barrier pair hands out
-// the global reservations. Every thread of the block calls it.
-constexpr uint32_t kCommitPerThread = 4;
+// the global reservations. Every thread of the block calls it. Kernels that
+// use it take kEntriesPerThread items per thread (a block's items in steps of
+// blockDim.x) and issue each step's loads for all of them before using any.
+constexpr uint32_t kEntriesPerThread = 4;
 
 __device__ __forceinline__ void blockReserveMany(BlockSlots& b, uint32_t* counters,
-                                                 const uint32_t (&key)[kCommitPerThread],
-                                                 uint32_t (&out)[kCommitPerThread]) {
+                                                 const uint32_t (&key)[kEntriesPerThread],
+                                                 uint32_t (&out)[kEntriesPerThread]) {
     const uint32_t lane = laneId();
-    uint32_t at[kCommitPerThread], off[kCommitPerThread], rank[kCommitPerThread];
+    uint32_t at[kEntriesPerThread], off[kEntriesPerThread], rank[kEntriesPerThread];
 #pragma unroll
-    for (uint32_t j = 0; j < kCommitPerThread; j++) {
+    for (uint32_t j = 0; j < kEntriesPerThread; j++) {
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, key[j]);
         const int leader = __ffs(peers) - 1;
         rank[j] = __popc(peers & ((1u << lane) - 1u));
@@ -1194,13 +1196,13 @@ __device__ __forceinline__ void blockReserveMany(BlockSlots& b, uint32_t* counte
     }
     __syncthreads();
 #pragma unroll
-    for (uint32_t j = 0; j < kCommitPerThread; j++)
+    for (uint32_t j = 0; j < kEntriesPerThread; j++)
         out[j] = key[j] == kNone ? kNone : (at[j] != kNone ? b.base[at[j]] : 0u) + off[j] + rank[j];
 }
 
 // Sets the new cells' bits and gives each new voxel its slot in its node
 // (sampleVoxel :119-138). Keys are unique, so every bit is set exactly once.
-// A thread takes kCommitPerThread list entries (a block's entries in steps of
+// A thread takes kEntriesPerThread list entries (a block's entries in steps of
 // blockDim.x) and issues each step's loads for all of them before using any,
 // so one iteration waits on three rounds of memory instead of three per entry.
 __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
@@ -1212,20 +1214,20 @@ __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
     const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
     const uint32_t per = (((nnew + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
     const uint32_t begin = min(nnew, blockIdx.x * per), end = min(nnew, begin + per);
-    for (uint32_t base = begin; base < end; base += blockDim.x * kCommitPerThread) {
-        uint32_t e[kCommitPerThread], slot[kCommitPerThread], node[kCommitPerThread];
-        ulonglong2 kv[kCommitPerThread];
+    for (uint32_t base = begin; base < end; base += blockDim.x * kEntriesPerThread) {
+        uint32_t e[kEntriesPerThread], slot[kEntriesPerThread], node[kEntriesPerThread];
+        ulonglong2 kv[kEntriesPerThread];
 #pragma unroll
-        for (uint32_t j = 0; j < kCommitPerThread; j++) {
+        for (uint32_t j = 0; j < kEntriesPerThread; j++) {
             e[j] = base + j * blockDim.x + threadIdx.x;
             slot[j] = e[j] < end ? d.hashNew[e[j]] : kNone;
         }
 #pragma unroll
-        for (uint32_t j = 0; j < kCommitPerThread; j++)
+        for (uint32_t j = 0; j < kEntriesPerThread; j++)
             kv[j] = slot[j] != kNone ? d.hashSlots[slot[j]] : make_ulonglong2(kHashEmpty, 0ull);
-        uint32_t g[kCommitPerThread];
+        uint32_t g[kEntriesPerThread];
 #pragma unroll
-        for (uint32_t j = 0; j < kCommitPerThread; j++) {
+        for (uint32_t j = 0; j < kEntriesPerThread; j++) {
             node[j] = kNone;
             g[j] = 0;
             if (slot[j] != kNone) {
@@ -1236,7 +1238,7 @@ __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
             }
         }
 #pragma unroll
-        for (uint32_t j = 0; j < kCommitPerThread; j++) {
+        for (uint32_t j = 0; j < kEntriesPerThread; j++) {
             if (node[j] == kNone) continue;
             const uint32_t vi = (uint32_t)(kv[j].x & 0x1FFFFFull);
             atomicOr(gridWordsAt(d, g[j]) + (vi >> 5), 1u << (vi & 31u));
@@ -1244,10 +1246,10 @@ __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
             d.hashNewCell[e[j]] = vi;
             d.hashNewColor[e[j]] = (uint32_t)(kv[j].y & 0xFFFFFFFFull);
         }
-        uint32_t s[kCommitPerThread];
+        uint32_t s[kEntriesPerThread];
         blockReserveMany(s_slots, d.numVoxels, node, s);
 #pragma unroll
-        for (uint32_t j = 0; j < kCommitPerThread; j++)
+        for (uint32_t j = 0; j < kEntriesPerThread; j++)
             if (node[j] != kNone) d.hashNewSlot[e[j]] = s[j];
     }
 }
@@ -1365,32 +1367,52 @@ __global__ void __launch_bounds__(256) k_insert(Dev d, const Point* __restrict__
     const uint32_t ppc = d.ppc;
     const uint32_t per = (((total + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
     const uint32_t begin = min(total, blockIdx.x * per), end = min(total, begin + per);
-    for (uint32_t base = begin; base < end; base += blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        uint32_t leaf = kNone, gidx = 0;
-        Point p = {0.f, 0.f, 0.f, 0u};
-        if (i >= end) {
-        } else if (i < n) {
-            leaf = d.leafOf[i];
-            p = loadPoint(pts + i);
-            gidx = firstIndex + i;
-        } else {
-            const uint32_t j = i - n;
-            leaf = d.spillLeaf[j];
-            p = d.spillPts[j];
-            gidx = d.spillIdx[j];
+    for (uint32_t base = begin; base < end; base += blockDim.x * kEntriesPerThread) {
+        uint32_t leaf[kEntriesPerThread], gidx[kEntriesPerThread];
+        Point p[kEntriesPerThread];
+#pragma unroll
+        for (uint32_t j = 0; j < kEntriesPerThread; j++) {
+            const uint32_t i = base + j * blockDim.x + threadIdx.x;
+            leaf[j] = kNone;
+            gidx[j] = 0;
+            p[j] = Point{0.f, 0.f, 0.f, 0u};
+            if (i >= end) {
+            } else if (i < n) {
+                leaf[j] = d.leafOf[i];
+                p[j] = loadPoint(pts + i);
+                gidx[j] = firstIndex + i;
+            } else {
+                leaf[j] = d.spillLeaf[i - n];
+                p[j] = d.spillPts[i - n];
+                gidx[j] = d.spillIdx[i - n];
+            }
         }
-        const uint32_t slot = blockReserve(s_slots, d.numPoints, leaf);
-        if (leaf == kNone) continue;
-        const uint32_t cap = d.numPointChunks[leaf] * ppc;
-        uint32_t phys = kNone;
-        if (slot < cap) phys = d.tablePool[d.ptTableOff[leaf] + slot / ppc];
-        if (phys == kNone) {
-            atomicAdd(reinterpret_cast<unsigned long long*>(&c->droppedPoints), 1ull);
-            continue;
+        uint32_t slot[kEntriesPerThread];
+        blockReserveMany(s_slots, d.numPoints, leaf, slot);
+        uint32_t cap[kEntriesPerThread], off[kEntriesPerThread];
+#pragma unroll
+        for (uint32_t j = 0; j < kEntriesPerThread; j++) {
+            cap[j] = 0;
+            off[j] = 0;
+            if (leaf[j] != kNone) {
+                cap[j] = d.numPointChunks[leaf[j]] * ppc;
+                off[j] = d.ptTableOff[leaf[j]];
+            }
         }
-        chunkPoints(d, phys)[slot % ppc] = p;
-        chunkIndices(d, phys)[slot % ppc] = gidx;
+        uint32_t phys[kEntriesPerThread];
+#pragma unroll
+        for (uint32_t j = 0; j < kEntriesPerThread; j++)
+            phys[j] = (leaf[j] != kNone && slot[j] < cap[j]) ? d.tablePool[off[j] + slot[j] / ppc] : kNone;
+#pragma unroll
+        for (uint32_t j = 0; j < kEntriesPerThread; j++) {
+            if (leaf[j] == kNone) continue;
+            if (phys[j] == kNone) {
+                atomicAdd(reinterpret_cast<unsigned long long*>(&c->droppedPoints), 1ull);
+                continue;
+            }
+            chunkPoints(d, phys[j])[slot[j] % ppc] = p[j];
+            chunkIndices(d, phys[j])[slot[j] % ppc] = gidx[j];
+        }
     }
 }
 

@@ -263,8 +263,9 @@ bool graphPath(rb_ctx* c) {
     return c->batchGraph != nullptr;
 }
 
-// Launches of one graph batch, for the per-kernel counts: eleven fixed
-// kernels per batch, four per pass of the expand loop.
+// Launches of graph batches, for the per-kernel counts: nine fixed kernels
+// and the loop test per batch, four kernels per expand pass, and four per
+// unrolled pass that ran after the loop ended (k_expand_skipped).
 void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint32_t skipsBefore, uint64_t points) {
     // every batch graph runs the loop test once after its first count and once
     // after each split pass; an unrolled pass after the loop ended launches its

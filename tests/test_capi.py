@@ -80,6 +80,10 @@ def test_create_validates_and_fails_loudly_without_gpu():
     h = ctypes.c_void_p()
     bad = capi.default_config(struct_size=4)
     assert lib.rb_create(ctypes.byref(bad), ctypes.byref(h)) == capi.RB_ERR_INVALID_ARG
+    # the cell table takes 2 x backlog_capacity 16-byte slots: 2^28 (8 GB) is the limit
+    bad = capi.default_config(backlog_capacity=(1 << 28) + 1)
+    assert lib.rb_create(ctypes.byref(bad), ctypes.byref(h)) == capi.RB_ERR_INVALID_ARG
+    assert c.backlog_capacity == 0  # 0: sized from slot_capacity
     st = lib.rb_create(ctypes.byref(c), ctypes.byref(h))
     import torch
     if torch.cuda.is_available():

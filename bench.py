@@ -137,13 +137,27 @@ def barrier(world):
         dist.barrier()
 
 
-def generate_cloud(seed, num_points):
+def generate_cloud(seed, num_points=None, count=None):
+    """Configuration 2's cloud for `seed` (num_points None: the configuration's
+    100M). count: only its first `count` points -- a prefix of the same cloud,
+    not a smaller cloud (the sensor path spans the configured size)."""
     from remobench_b200 import synth
-    cfg = synth.config(2, seed=seed, num_points=num_points)
+    over = {"seed": seed}
+    if num_points is not None:
+        over["num_points"] = num_points
+    cfg = synth.config(2, **over)
     t0 = time.time()
-    pts = synth.generate(cfg)
+    pts = synth.generate(cfg, 0, count)
     bmin, bmax = synth.scene_box(cfg)
     return cfg, pts, bmin, bmax, time.time() - t0
+
+
+def sample_identity(pts, sample_batches):
+    """Which points a CPU sample covers: its first batch, count and a digest."""
+    import hashlib
+    n = min(len(pts), sample_batches * BATCH)
+    h = hashlib.blake2b(np.ascontiguousarray(pts[:n]).view(np.uint8), digest_size=8).hexdigest()
+    return {"first_batch": 0, "batches": sample_batches, "points": int(n), "blake2b_64": h}
 
 
 def cpu_baseline(pts, bmin, bmax, sample_batches, threads):
@@ -165,31 +179,66 @@ def cpu_baseline(pts, bmin, bmax, sample_batches, threads):
     return n / dt / 1e6, dt, n
 
 
+def cpu_baseline_median(pts, bmin, bmax, sample_batches, threads, reps):
+    """Median Mpts/s of `reps` runs of cpu_baseline, and the last run's time."""
+    vals, dt = [], 0.0
+    for _ in range(max(reps, 1)):
+        v, dt, _ = cpu_baseline(pts, bmin, bmax, sample_batches, threads)
+        vals.append(v)
+    return statistics.median(vals), dt
+
+
+def reference_kernels_b200(pts, bmin, bmax):
+    """The reference's own kernels (kernels/remolod, NVRTC-compiled from its
+    sources into oracle/_ref/ in the build container) timed on this GPU over
+    the same cloud; None when they were not built or no GPU is visible."""
+    lib = os.path.join(ROOT, "oracle", "_ref", "libref_launcher.so")
+    if not os.path.exists(lib):
+        return {"unavailable": "oracle/_ref was not built (the reference sources are not mounted here)"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+        sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+        from time_ref import time_kernels
+        return time_kernels(pts, bmin, bmax, BATCH, "shipped")
+    except Exception as e:  # reported, not fatal: the CPU arm stands on its own
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
 def run_reference(args, world, rank):
     """--impl reference: the reference path's CPU implementation (the oracle
     port; the reference's own code is GPU-only and GL-bound) on a bounded sample
-    of the same workload, every host thread it can use."""
+    of the same workload -- the first cpu_sample_batches batches of the 100M
+    cloud the repo arm ingests -- every host thread it can use. The reference's
+    own GPU kernels, timed on the same box over the whole cloud, ride along as
+    reference_kernels_b200 (not the line's value)."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     sample = args.cpu_sample_batches
-    cfg, pts, bmin, bmax, _ = generate_cloud(1, sample * BATCH)
+    cfg, pts, bmin, bmax, _ = generate_cloud(1, count=sample * BATCH)
     for _ in range(args.warmup):
         cpu_baseline(pts, bmin, bmax, min(sample, 2), threads)
-    vals = []
-    for _ in range(args.steps):
-        v, dt, n = cpu_baseline(pts, bmin, bmax, sample, threads)
-        vals.append(v)
-    value = statistics.median(vals)
+    value, dt = cpu_baseline_median(pts, bmin, bmax, sample, threads, args.steps)
+    ident = sample_identity(pts, sample)
+    kernels = None
+    if not args.no_reference_kernels:
+        del pts
+        _, full, bmin, bmax, _ = generate_cloud(1)
+        kernels = reference_kernels_b200(full, bmin, bmax)
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 points, int64 sums", "data": "synthetic",
             "config": {"workload": f"config 2 sample: first {sample} x 1M-point batches of the 100M-point "
                                    "2x2 km synthetic lidar cloud, Update+Accumulate",
-                       "batch_points": BATCH},
+                       "batch_points": BATCH, "sample": ident},
             "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{sample} x 1M-point batches, the restatement on {threads} threads"},
-            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                             "sample": f"first {sample} x 1M-point batches of the 100M-point cloud "
+                                       f"(median of {args.steps} runs, {dt:.1f} s each), the restatement "
+                                       f"on {threads} threads", "identity": ident},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_kernels_b200": kernels}
     print(json.dumps(line), flush=True)
 
 
@@ -203,6 +252,9 @@ def main():
     ap.add_argument("--frames", type=int, default=30)
     ap.add_argument("--cpu-sample-batches", type=int, default=20)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-reps", type=int, default=3)
+    ap.add_argument("--no-reference-kernels", action="store_true",
+                    help="reference arm: skip timing the reference's own GPU kernels")
     args = ap.parse_args()
 
     world, rank, local = dist_setup()
@@ -220,7 +272,7 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    cfg, pts, bmin, bmax, gen_s = generate_cloud(1 + rank, args.points)
+    cfg, pts, bmin, bmax, gen_s = generate_cloud(1 + rank, args.points if args.points != 100_000_000 else None)
     n = len(pts)
     nb = (n + BATCH - 1) // BATCH
 
@@ -347,10 +399,12 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample_batches > 0:
         threads = os.cpu_count() or 1
-        v, dt, npts = cpu_baseline(pts, bmin, bmax, args.cpu_sample_batches, threads)
+        v, dt = cpu_baseline_median(pts, bmin, bmax, args.cpu_sample_batches, threads, args.cpu_reps)
         cpu = {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"first {args.cpu_sample_batches} x 1M-point batches of the same cloud, "
-                         f"Update+Accumulate, {dt:.1f} s on {threads} threads"}
+                         f"Update+Accumulate, median of {args.cpu_reps} runs ({dt:.1f} s each) on "
+                         f"{threads} threads",
+               "identity": sample_identity(pts, args.cpu_sample_batches)}
 
     if rank == 0:
         p50 = float(np.percentile(frame_ms, 50)) if frame_ms else None

@@ -91,7 +91,13 @@ typedef struct rb_config {
                                         more often than the default's 64 MB at 1M-point slots. A batch with more
                                         new cells keeps the first ones and sets RB_OVF_BACKLOG, as the reference
                                         does at its limit. */
-    uint32_t reserved[6];
+    uint64_t store_capacity;         /* 0: the reference store's capacity is sized from the cloud and the
+                                        budget as RemolodPipeline::allocate does (48 B/pt, 512 MB floor,
+                                        RemolodPipeline.cpp:118-157); else exactly this many bytes, for a
+                                        caller with its own sizing (ref_alloc's persistent size). The
+                                        memory check (remolod_octree.cu:1181-1210) stops at offset +
+                                        safety_margin >= store_capacity. */
+    uint32_t reserved[4];
 } rb_config;
 
 /* CloudMeta (include/remo/PointSource.h:16-32), headless subset. */
@@ -272,20 +278,21 @@ rb_status rb_accumulate(struct rb_ctx* ctx, uint32_t batch_index, rb_accum_globa
 rb_status rb_render(struct rb_ctx* ctx, const rb_frame* frame, uint64_t fb_dev, uint64_t rgba_dev,
                     uint64_t force_large_dev, rb_render_result* out);
 
-/* rb_render without any allocation. No counterpart in the reference: its
- * render allocates nothing per frame only because the pipeline sized one
- * scratch buffer up front (RemolodPipeline.cpp:543-557), and its EDL pass runs
- * inside the same kernel. This entry point is for callers that build the tree
- * ahead of time but must render where they cannot allocate: a frame callback
- * with a hard real-time budget that may not take the allocator's lock or risk
- * an allocation failure mid-frame, or an embedder whose own pool owns all
- * device memory after start-up. It calls no cudaMalloc/cudaFree; its scratch
- * (per-node flags, the draw list, three counters) is a static device array of
- * about 1 MB that every GPU loading this library holds until exit. Limits:
- * max_nodes <= 262144 and drawlist_capacity <= 131072, else RB_ERR_CAPACITY.
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture. Calls share
- * the array: calls that overlap on the GPU race. Output equals rb_render's. */
+/* rb_render without any allocation; it has no counterpart in the reference.
+ * It is for callers that build the tree ahead of time but must render where
+ * they cannot allocate: a frame callback with a hard real-time budget that may
+ * not take the allocator's lock or risk an allocation failure mid-frame, or an
+ * embedder whose own pool owns all device memory after start-up. It calls no
+ * cudaMalloc/cudaFree; its scratch (per-node flags, the draw list, three
+ * counters) is a static device array of about 1 MB. rb_allocate resolves the
+ * array's device address (cudaGetSymbolAddress, with the context's device
+ * current), which under lazy module loading is also when the array is
+ * reserved on that device; it stays reserved until the process exits, so
+ * every rb_render_noalloc call is allocation-free. Limits: max_nodes <= 262144
+ * and drawlist_capacity <= 131072, else RB_ERR_CAPACITY. Calls share the
+ * array: calls that overlap on the GPU race. The caller's current device is
+ * restored before return. A context allocated before a cudaDeviceReset must
+ * not be used after it. Output equals rb_render's. */
 rb_status rb_render_noalloc(struct rb_ctx* ctx, const rb_frame* frame, uint64_t fb_dev, uint64_t rgba_dev,
                             uint64_t force_large_dev, rb_render_result* out);
 

@@ -1,10 +1,11 @@
 """Builds the reference's own kernels and a headless launcher into oracle/_ref/.
 
 Test infrastructure only: the outputs are the reference, run on the GPU to pin
-the CPU oracle. Reads the reference sources where they lie (/root/reference,
-read-only, present only in the build container); writes only oracle/_ref/.
+the CPU oracle. Reads the reference sources where they lie (a read-only tree,
+present only in the build container: pass its root with --reference or the
+REMOBENCH_REFERENCE environment variable); writes only oracle/_ref/.
 
-  python oracle/ref/build_ref.py [--reference /root/reference]
+  python oracle/ref/build_ref.py --reference <reference root>
 
 Two variants of each module (kernels/remolod/remolod_{reset,octree,accum,render}.cu):
   shipped -- the reference's NVRTC options verbatim (--use_fast_math, LTO link)
@@ -23,9 +24,12 @@ MODULES = ["remolod_reset", "remolod_octree", "remolod_accum", "remolod_render"]
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("REMOBENCH_REFERENCE"),
+                    help="root of the reference source tree (or set REMOBENCH_REFERENCE)")
     args = ap.parse_args()
     ref = args.reference
+    if not ref:
+        ap.error("the reference root is required: --reference or REMOBENCH_REFERENCE")
     if not os.path.isdir(os.path.join(ref, "kernels", "remolod")):
         print(f"reference sources not found under {ref}; nothing to build", file=sys.stderr)
         return 1

@@ -30,7 +30,7 @@ class Config(ctypes.Structure):
                 ("time_budget_ms", f32), ("voxel_mode", u32), ("accumulate", u32),
                 ("spilled_capacity", u32), ("spilling_nodes_capacity", u32), ("drawlist_capacity", u32),
                 ("safety_margin", u64), ("use_graphs", u32), ("backlog_capacity", u32),
-                ("reserved", u32 * 6)]
+                ("store_capacity", u64), ("reserved", u32 * 4)]
 
 
 class CloudMeta(ctypes.Structure):

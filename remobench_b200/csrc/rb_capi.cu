@@ -13,6 +13,7 @@
 
 #include "../../include/rb_capi.h"
 #include "rb_analysis.h"
+#include "rb_ctx_access.h"
 #include "rb_kernels.h"
 #include "rb_mlp.h"
 #include "rb_state.h"
@@ -484,6 +485,14 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
                         std::to_string(available >> 20) + " MB available");
     uint64_t want = std::max<uint64_t>((uint64_t)(48.0 * (double)meta->num_points), minPersistent);
     d.persistentCapacity = std::min<uint64_t>(want, available - fixedBytes);
+    if (cfg.store_capacity) {
+        // a caller-sized store (the reference launcher's persistent size)
+        if (cfg.store_capacity > available - fixedBytes)
+            return fail(c, RB_ERR_OUT_OF_MEMORY,
+                        "store_capacity " + std::to_string(cfg.store_capacity >> 20) + " MB exceeds the " +
+                            std::to_string((available - fixedBytes) >> 20) + " MB the budget leaves");
+        d.persistentCapacity = cfg.store_capacity;
+    }
 
     // The arena: the reference store's worst case plus the wider point chunks
     // (indices kept beside the points): at most 1.25 x its capacity.
@@ -595,6 +604,9 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
         RB_CUDA(c, cudaEventCreateWithFlags(&c->slotFull[i], cudaEventDisableTiming));
     }
     RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    // the allocation-free render's static scratch is reserved here, where
+    // allocating is expected, not at its first call
+    RB_CUDA(c, rb::noallocPrepare(c->device));
     c->allocated = true;
     return rb_reset(c);
 }

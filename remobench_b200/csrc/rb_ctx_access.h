@@ -32,5 +32,9 @@ bool ctxRenderAccess(rb_ctx* ctx, CtxRenderAccess* out);
 void ctxSetError(rb_ctx* ctx, const char* msg);
 // Records the last render's visible node and sample counts for rb_read_stats.
 void ctxNoteVisible(rb_ctx* ctx, uint32_t nodes, uint64_t samples);
+// Resolves the allocation-free render's static scratch on `device` (which must
+// be current); rb_allocate calls it so that rb_render_noalloc never loads a
+// module or reserves memory itself (rb_noalloc.cu).
+cudaError_t noallocPrepare(int device);
 
 }  // namespace rb

@@ -10,14 +10,21 @@
 // this entry point does neither.
 //
 // Its scratch -- per-node visible/large flags, the draw list and the three
-// counters -- is one file-scope __device__ array of kScratchBytes (about 1 MB),
-// which every GPU that loads this library holds until the process exits. Host
-// code cannot use the array's name as a device address (on the host it names
-// a host-side stand-in), so the first call on each device, with that device
+// counters -- is one file-scope __device__ array of kScratchBytes (about 1 MB).
+// Host code cannot use the array's name as a device address (on the host it
+// names a host-side stand-in), so rb_allocate, with the context's device
 // current, asks the runtime for the array's device address with
-// cudaGetSymbolAddress and keeps it. Make that first call before any stream
-// capture. All calls share the array and it keeps the last call's contents:
-// the counters are cleared by the first kernel of every call, and the flags and
+// cudaGetSymbolAddress and keeps it per device (noallocPrepare below). Under
+// lazy module loading that lookup is also what loads this file's module and
+// reserves the array on the device, so the reservation happens inside
+// rb_allocate -- where allocation is expected -- and every rb_render_noalloc
+// call afterwards is allocation-free. The array then stays reserved on that
+// device until the process exits. Every rb_allocate looks the address up again,
+// so a context allocated after a cudaDeviceReset gets the reloaded module's
+// address; a context allocated before a reset must not be used after it.
+//
+// All calls share the array and it keeps the last call's contents: the
+// counters are cleared by the first kernel of every call, and the flags and
 // the draw list are written before they are read. Calls that overlap on the
 // GPU (two streams, two contexts on one device) race on the array.
 //
@@ -54,31 +61,94 @@ constexpr int kMaxDevices = 128;
 std::mutex g_scratchMutex;
 unsigned char* g_scratchAddr[kMaxDevices] = {};
 
-// The array's device address on `device`, which must be current.
-rb_status scratchAddress(rb_ctx* ctx, int device, unsigned char** out) {
-    if (device < 0 || device >= kMaxDevices) {
-        rb::ctxSetError(ctx, "rb_render_noalloc: device ordinal out of range");
-        return RB_ERR_INVALID_ARG;
+// Looks the array's device address up on `device`, which must be current,
+// and keeps it. Called by rb_allocate (see noallocPrepare).
+cudaError_t resolveScratch(int device) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_renderScratch);
+    if (e != cudaSuccess || p == nullptr) {
+        cudaGetLastError();
+        return e != cudaSuccess ? e : cudaErrorInvalidSymbol;
     }
     std::lock_guard<std::mutex> lock(g_scratchMutex);
-    if (!g_scratchAddr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_renderScratch);
-        if (e != cudaSuccess || p == nullptr) {
-            cudaGetLastError();
-            rb::ctxSetError(ctx, (std::string("rb_render_noalloc: cudaGetSymbolAddress failed: ") +
-                                  cudaGetErrorString(e)).c_str());
-            return RB_ERR_CUDA;
-        }
-        g_scratchAddr[device] = static_cast<unsigned char*>(p);
-    }
-    *out = g_scratchAddr[device];
-    return RB_OK;
+    g_scratchAddr[device] = static_cast<unsigned char*>(p);
+    return cudaSuccess;
+}
+
+// The address rb_allocate resolved for `device`, or null.
+unsigned char* scratchAddress(int device) {
+    if (device < 0 || device >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(g_scratchMutex);
+    return g_scratchAddr[device];
 }
 
 rb_status cudaFail(rb_ctx* ctx, const char* what, cudaError_t e) {
     rb::ctxSetError(ctx, (std::string("rb_render_noalloc: ") + what + ": " + cudaGetErrorString(e)).c_str());
     return RB_ERR_CUDA;
+}
+
+}  // namespace
+
+namespace rb {
+
+cudaError_t noallocPrepare(int device) {
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    return resolveScratch(device);
+}
+
+}  // namespace rb
+
+namespace {
+
+// The render itself, with the context's device current.
+rb_status renderNoalloc(rb_ctx* ctx, const rb::CtxRenderAccess& a, unsigned char* base, const rb_frame* f,
+                        uint64_t fbDev, uint64_t rgbaDev, uint64_t forceDev, uint32_t cap, rb_render_result* out) {
+    uint8_t* vis = base + kOffVis;
+    uint8_t* large = base + kOffLarge;
+    uint32_t* items = reinterpret_cast<uint32_t*>(base + kOffItems);
+    rb::RenderScratch* rs = reinterpret_cast<rb::RenderScratch*>(base + kOffCounters);
+
+    const uint64_t npx = (uint64_t)f->width * (uint64_t)f->height;
+    auto* fb = reinterpret_cast<unsigned long long*>(fbDev);
+    rb::Frame fr;
+    fr.width = f->width;
+    fr.height = f->height;
+    std::memcpy(fr.transform, f->transform, sizeof(fr.transform));
+    std::memcpy(fr.transformFrozen, f->transform_frozen, sizeof(fr.transformFrozen));
+    for (int k = 0; k < 3; k++) {
+        fr.boxMin[k] = f->box_min[k];
+        fr.boxMax[k] = f->box_max[k];
+    }
+    fr.lodPixelBudget = f->lod_pixel_budget;
+    fr.pointSize = f->point_size;
+
+    cudaError_t e;
+    cudaStream_t s = a.stream;
+    if ((e = cudaEventRecord(a.evStart, s)) != cudaSuccess) return cudaFail(ctx, "cudaEventRecord", e);
+    rb::launchFbClear(fb, npx, a.numSMs * 8, s);
+    // the first kernel zeroes the counter block (draw items, overflow, samples)
+    rb::launchNodeFlags(a.d, fr, vis, large, reinterpret_cast<const uint8_t*>(forceDev), rs, a.numSMs * 4, s);
+    rb::launchFrontier(a.d, vis, large, rs, items, cap, a.numSMs * 4, s);
+    rb::launchRaster(a.d, fr, fb, rs, items, cap, a.numSMs * 8, s);
+    if (f->enable_edl) rb::launchEdl(fb, fb, (uint32_t)f->width, (uint32_t)f->height, f->edl_strength,
+                                     a.numSMs * 8, s);
+    if (rgbaDev) rb::launchResolve(fb, reinterpret_cast<uint32_t*>(rgbaDev), npx, a.numSMs * 8, s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cudaFail(ctx, "kernel launch", e);
+    if ((e = cudaEventRecord(a.evStop, s)) != cudaSuccess) return cudaFail(ctx, "cudaEventRecord", e);
+    if ((e = cudaMemcpyAsync(a.hostRs, rs, sizeof(rb::RenderScratch), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cudaFail(ctx, "cudaMemcpyAsync", e);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(ctx, "cudaStreamSynchronize", e);
+    rb::ctxNoteVisible(ctx, a.hostRs->numItems, a.hostRs->samples);
+    if (out) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a.evStart, a.evStop);
+        out->draw_items = a.hostRs->numItems;
+        out->drawlist_overflow = a.hostRs->overflow;
+        out->draw_samples = a.hostRs->samples;
+        out->device_ms = ms;
+        out->pad = 0;
+    }
+    return RB_OK;
 }
 
 }  // namespace
@@ -113,54 +183,18 @@ extern "C" rb_status rb_render_noalloc(rb_ctx* ctx, const rb_frame* f, uint64_t 
         rb::ctxSetError(ctx, msg);
         return RB_ERR_CAPACITY;
     }
-    cudaError_t e = cudaSetDevice(a.device);
-    if (e != cudaSuccess) return cudaFail(ctx, "cudaSetDevice", e);
-    unsigned char* base = nullptr;
-    rb_status st = scratchAddress(ctx, a.device, &base);
-    if (st != RB_OK) return st;
-    uint8_t* vis = base + kOffVis;
-    uint8_t* large = base + kOffLarge;
-    uint32_t* items = reinterpret_cast<uint32_t*>(base + kOffItems);
-    rb::RenderScratch* rs = reinterpret_cast<rb::RenderScratch*>(base + kOffCounters);
-
-    const uint64_t npx = (uint64_t)f->width * (uint64_t)f->height;
-    auto* fb = reinterpret_cast<unsigned long long*>(fbDev);
-    rb::Frame fr;
-    fr.width = f->width;
-    fr.height = f->height;
-    std::memcpy(fr.transform, f->transform, sizeof(fr.transform));
-    std::memcpy(fr.transformFrozen, f->transform_frozen, sizeof(fr.transformFrozen));
-    for (int k = 0; k < 3; k++) {
-        fr.boxMin[k] = f->box_min[k];
-        fr.boxMax[k] = f->box_max[k];
+    unsigned char* base = scratchAddress(a.device);
+    if (!base) {
+        rb::ctxSetError(ctx, "rb_render_noalloc: the scratch array's address was not resolved; rb_allocate does it");
+        return RB_ERR_STATE;
     }
-    fr.lodPixelBudget = f->lod_pixel_budget;
-    fr.pointSize = f->point_size;
-
-    cudaStream_t s = a.stream;
-    if ((e = cudaEventRecord(a.evStart, s)) != cudaSuccess) return cudaFail(ctx, "cudaEventRecord", e);
-    rb::launchFbClear(fb, npx, a.numSMs * 8, s);
-    // the first kernel zeroes the counter block (draw items, overflow, samples)
-    rb::launchNodeFlags(a.d, fr, vis, large, reinterpret_cast<const uint8_t*>(forceDev), rs, a.numSMs * 4, s);
-    rb::launchFrontier(a.d, vis, large, rs, items, cap, a.numSMs * 4, s);
-    rb::launchRaster(a.d, fr, fb, rs, items, cap, a.numSMs * 8, s);
-    if (f->enable_edl) rb::launchEdl(fb, fb, (uint32_t)f->width, (uint32_t)f->height, f->edl_strength,
-                                     a.numSMs * 8, s);
-    if (rgbaDev) rb::launchResolve(fb, reinterpret_cast<uint32_t*>(rgbaDev), npx, a.numSMs * 8, s);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cudaFail(ctx, "kernel launch", e);
-    if ((e = cudaEventRecord(a.evStop, s)) != cudaSuccess) return cudaFail(ctx, "cudaEventRecord", e);
-    if ((e = cudaMemcpyAsync(a.hostRs, rs, sizeof(rb::RenderScratch), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-        return cudaFail(ctx, "cudaMemcpyAsync", e);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cudaFail(ctx, "cudaStreamSynchronize", e);
-    rb::ctxNoteVisible(ctx, a.hostRs->numItems, a.hostRs->samples);
-    if (out) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, a.evStart, a.evStop);
-        out->draw_items = a.hostRs->numItems;
-        out->drawlist_overflow = a.hostRs->overflow;
-        out->draw_samples = a.hostRs->samples;
-        out->device_ms = ms;
-        out->pad = 0;
-    }
-    return RB_OK;
+    // the caller's current device is put back on every return
+    int callerDevice = -1;
+    cudaError_t e = cudaGetDevice(&callerDevice);
+    if (e != cudaSuccess) return cudaFail(ctx, "cudaGetDevice", e);
+    if (callerDevice != a.device && (e = cudaSetDevice(a.device)) != cudaSuccess)
+        return cudaFail(ctx, "cudaSetDevice", e);
+    const rb_status st = renderNoalloc(ctx, a, base, f, fbDev, rgbaDev, forceDev, cap, out);
+    if (callerDevice != a.device) cudaSetDevice(callerDevice);
+    return st;
 }

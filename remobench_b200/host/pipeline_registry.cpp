@@ -1,166 +1,200 @@
-// The registry's gate arithmetic and switch sequence follow
-// src/shell/PipelineRegistry.cpp:20-274 step for step, so a cloud/budget pair
-// is refused, warned about or accepted exactly as the reference decides.
+// The pipeline registry: registration, the memory gate and pipeline switches.
+//
+// The gate decides, before any device memory is touched, whether a pipeline
+// may run a cloud in a byte budget, and how much of the cloud it will hold.
+// Its decisions are the reference registry's (src/shell/PipelineRegistry.cpp:
+// 20-274), restated here from these rules:
+//
+//   feed     bytes of point input the pipeline keeps on the device: the whole
+//            cloud at 16 B a point for a resident feed, else a ring of
+//            min(ringSlots, batches in the cloud) slots of kSlotCapacity points;
+//   need     what the whole cloud takes: minBytesPerPoint x points + feed +
+//            the pipeline's fixed buffers;
+//   floor    the smallest budget it runs in at all: `need` for a pipeline that
+//            cannot stop on a partial tree (minStoreBytes == 0), else its
+//            smallest store + feed + fixed buffers;
+//   fraction of the cloud predicted to fit: the store is the pipeline's
+//            appetite (bytesPerPoint x points) capped by what the budget
+//            leaves after feed and fixed buffers; ingest stops kSafetyMargin
+//            short of the store's end, and each stored point costs
+//            minBytesPerPoint (so a small cloud is predicted at 0% although
+//            allocate() would raise its store to the 512 MB floor -- kept, as
+//            the reference predicts it);
+//   ceiling  a resident feed to a progressive builder can only describe
+//            kRingDepth batches, because the builder finds batch b at slot
+//            b mod kRingDepth.
+//
+// A switch gates first, then releases the running pipeline, re-shapes the
+// point source for the incoming one (both share the budget), and brings the
+// incoming pipeline up: create, initPrograms, allocate, reset.
 #include "pipeline_registry.h"
 
 #include <algorithm>
+#include <cstdarg>
 #include <cstdio>
 
 namespace rbhost {
 
+namespace {
+
+double gigabytes(uint64_t bytes) { return static_cast<double>(bytes) / 1e9; }
+
+std::string format(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    return buf;
+}
+
+// Every figure the gate derives for one (pipeline, cloud, budget).
+struct GateFigures {
+    uint64_t feed = 0;       // device bytes of point input
+    uint64_t need = 0;       // budget that holds the whole cloud
+    uint64_t floor = 0;      // budget below which the pipeline is refused
+    bool fits = false;
+    double fraction = 0.0;   // predicted share of the cloud ingested
+};
+
+bool streams(const PipelineInfo& info) { return !info.needsWholeCloudResident && info.ringSlots > 0; }
+
+PointSource::Mode feedMode(const PipelineInfo* info) {
+    return (info == nullptr || info->needsWholeCloudResident) ? PointSource::Mode::Whole : PointSource::Mode::Stream;
+}
+
+GateFigures gate(const PipelineInfo& info, const CloudMeta& meta, uint64_t budget) {
+    GateFigures g;
+    g.feed = inputBytesFor(info, meta);
+    const uint64_t overhead = g.feed + info.fixedBytesEstimate;
+    g.need = static_cast<uint64_t>(info.minBytesPerPointEstimate * static_cast<double>(meta.numPoints)) + overhead;
+    const bool truncates = info.minStoreBytes != 0;
+    g.floor = truncates ? info.minStoreBytes + overhead : g.need;
+    g.fits = g.floor <= budget;
+    if (meta.numPoints == 0) {
+        g.fraction = 1.0;
+    } else if (info.minBytesPerPointEstimate <= 0.0) {
+        g.fraction = g.fits ? 1.0 : 0.0;  // no per-point store: all or nothing
+    } else if (budget > overhead) {
+        const uint64_t appetite =
+            static_cast<uint64_t>(info.bytesPerPointEstimate * static_cast<double>(meta.numPoints));
+        const uint64_t store = std::min(appetite, budget - overhead);
+        const uint64_t usable = store > kPersistentSafetyMargin ? store - kPersistentSafetyMargin : 0;
+        const double storedPoints = static_cast<double>(usable) / info.minBytesPerPointEstimate;
+        g.fraction = std::clamp(storedPoints / static_cast<double>(meta.numPoints), 0.0, 1.0);
+    }
+    return g;
+}
+
+}  // namespace
+
+uint64_t inputBytesFor(const PipelineInfo& info, const CloudMeta& meta) {
+    constexpr uint64_t kPointBytes = sizeof(rb_point);
+    if (!streams(info)) return meta.numPoints * kPointBytes;
+    const uint64_t batches = (meta.numPoints + kSlotCapacity - 1) / kSlotCapacity;
+    return std::min<uint64_t>(info.ringSlots, batches) * kSlotCapacity * kPointBytes;
+}
+
 void PipelineRegistry::add(PipelineFactory factory) {
-    if (!factory) return;
-    std::unique_ptr<ILodPipeline> probe = factory();
-    if (!probe) {
-        std::fprintf(stderr, "rbhost: pipeline factory returned null at registration\n");
+    // a throwaway instance tells the registry what the factory makes
+    std::unique_ptr<ILodPipeline> sample = factory ? factory() : nullptr;
+    if (!sample) {
+        std::fprintf(stderr, "rbhost: registration skipped: the factory is empty or made no pipeline\n");
         return;
     }
-    PipelineInfo info = probe->info();
-    probe.reset();
-    if (info.id.empty()) {
-        std::fprintf(stderr, "rbhost: pipeline has an empty id; not registered\n");
-        return;
-    }
-    if (find(info.id)) {
-        std::fprintf(stderr, "rbhost: duplicate pipeline id '%s'; not registered\n", info.id.c_str());
+    PipelineInfo info = sample->info();
+    sample.reset();
+    const char* why = info.id.empty() ? "it has no id" : (find(info.id) ? "its id is taken" : nullptr);
+    if (why) {
+        std::fprintf(stderr, "rbhost: pipeline '%s' not registered: %s\n", info.id.c_str(), why);
         return;
     }
     m_infos.push_back(info);
-    m_entries.push_back({std::move(info), std::move(factory)});
+    m_entries.push_back(Entry{std::move(info), std::move(factory)});
 }
 
 const PipelineInfo* PipelineRegistry::find(const std::string& id) const {
-    for (const Entry& e : m_entries)
-        if (e.info.id == id) return &e.info;
-    return nullptr;
-}
-
-uint64_t inputBytesFor(const PipelineInfo& info, const CloudMeta& meta) {
-    if (!info.needsWholeCloudResident && info.ringSlots > 0) {
-        const uint64_t total = (meta.numPoints + kSlotCapacity - 1) / kSlotCapacity;
-        const uint64_t slots = std::min<uint64_t>(info.ringSlots, total);
-        return slots * kSlotCapacity * sizeof(rb_point);
-    }
-    return meta.numPoints * sizeof(rb_point);
+    const auto it = std::find_if(m_entries.begin(), m_entries.end(), [&](const Entry& e) { return e.info.id == id; });
+    return it == m_entries.end() ? nullptr : &it->info;
 }
 
 uint64_t PipelineRegistry::minBytesRequired(const PipelineInfo& info, const CloudMeta& meta) const {
-    const double perPoint = info.minBytesPerPointEstimate * static_cast<double>(meta.numPoints);
-    return static_cast<uint64_t>(perPoint) + inputBytesFor(info, meta) + info.fixedBytesEstimate;
+    return gate(info, meta, 0).need;
 }
 
 uint64_t PipelineRegistry::refusalFloor(const PipelineInfo& info, const CloudMeta& meta) const {
-    // A pipeline that truncates cleanly is refused only when it cannot run at all.
-    if (info.minStoreBytes == 0) return minBytesRequired(info, meta);
-    return info.minStoreBytes + inputBytesFor(info, meta) + info.fixedBytesEstimate;
+    return gate(info, meta, 0).floor;
 }
 
 bool PipelineRegistry::fits(const PipelineInfo& info, const CloudMeta& meta, const DeviceBudget& budget) const {
-    return refusalFloor(info, meta) <= budget.bytes;
+    return gate(info, meta, budget.bytes).fits;
 }
 
 double PipelineRegistry::predictedCompletion(const PipelineInfo& info, const CloudMeta& meta,
                                              const DeviceBudget& budget) const {
-    if (meta.numPoints == 0) return 1.0;
-    if (info.minBytesPerPointEstimate <= 0.0) return fits(info, meta, budget) ? 1.0 : 0.0;
-    const uint64_t overhead = inputBytesFor(info, meta) + info.fixedBytesEstimate;
-    if (budget.bytes <= overhead) return 0.0;
-    const uint64_t room = budget.bytes - overhead;
-    const uint64_t want = static_cast<uint64_t>(info.bytesPerPointEstimate * static_cast<double>(meta.numPoints));
-    const uint64_t persistent = std::min(want, room);
-    const uint64_t usable = persistent > kPersistentSafetyMargin ? persistent - kPersistentSafetyMargin : 0;
-    const double points = static_cast<double>(usable) / info.minBytesPerPointEstimate;
-    return std::clamp(points / static_cast<double>(meta.numPoints), 0.0, 1.0);
+    return gate(info, meta, budget.bytes).fraction;
 }
 
 std::string PipelineRegistry::completionWarning(const PipelineInfo& info, const CloudMeta& meta,
                                                 const DeviceBudget& budget) const {
-    const double fraction = predictedCompletion(info, meta, budget);
-    if (fraction >= 0.999) return {};
-    char buf[256];
-    std::snprintf(buf, sizeof(buf),
-                  "the budget holds about %.0f%% of this cloud; ingest will stop cleanly on a truncated tree "
-                  "(memCapacityReached). %.1f GB of budget would hold all of it.",
-                  fraction * 100.0, static_cast<double>(minBytesRequired(info, meta)) / 1e9);
-    return buf;
+    const GateFigures g = gate(info, meta, budget.bytes);
+    if (g.fraction >= 0.999) return {};
+    return format("predicted to take in about %.0f%% of the cloud before its store fills; the build then ends on "
+                  "a partial tree (memCapacityReached). The whole cloud needs a %.1f GB budget.",
+                  g.fraction * 100.0, gigabytes(g.need));
 }
 
 std::string PipelineRegistry::unsupportedReason(const PipelineInfo& info, const CloudMeta& meta,
                                                 const DeviceBudget& budget) const {
-    if (!fits(info, meta, budget)) {
-        const double inputGB = static_cast<double>(inputBytesFor(info, meta)) / 1e9;
-        const char* input = info.needsWholeCloudResident ? "resident cloud" : "ring";
-        char buf[384];
-        if (info.minStoreBytes == 0) {
-            std::snprintf(buf, sizeof(buf),
-                          "needs %.1f GB for %llu points and cannot build a partial tree (%.0f B/pt structure + "
-                          "%.1f GB %s + %.2f GB fixed); the budget is %.1f GB",
-                          static_cast<double>(minBytesRequired(info, meta)) / 1e9,
-                          static_cast<unsigned long long>(meta.numPoints), info.minBytesPerPointEstimate, inputGB,
-                          input, static_cast<double>(info.fixedBytesEstimate) / 1e9,
-                          static_cast<double>(budget.bytes) / 1e9);
-        } else {
-            std::snprintf(buf, sizeof(buf),
-                          "cannot run at all below %.1f GB (%.1f GB %s + %.2f GB fixed + %.2f GB smallest store); "
-                          "the budget is %.1f GB. The whole cloud would need %.1f GB.",
-                          static_cast<double>(refusalFloor(info, meta)) / 1e9, inputGB, input,
-                          static_cast<double>(info.fixedBytesEstimate) / 1e9,
-                          static_cast<double>(info.minStoreBytes) / 1e9, static_cast<double>(budget.bytes) / 1e9,
-                          static_cast<double>(minBytesRequired(info, meta)) / 1e9);
-        }
-        return buf;
+    const GateFigures g = gate(info, meta, budget.bytes);
+    const char* feedName = info.needsWholeCloudResident ? "resident cloud" : "ring";
+    if (!g.fits && info.minStoreBytes == 0) {
+        return format("refused: the whole cloud (%llu points) needs %.1f GB -- %.0f B per point, a %.1f GB %s and "
+                      "%.2f GB of fixed buffers -- and this pipeline cannot stop on a partial tree; the budget is "
+                      "%.1f GB",
+                      static_cast<unsigned long long>(meta.numPoints), gigabytes(g.need),
+                      info.minBytesPerPointEstimate, gigabytes(g.feed), feedName,
+                      gigabytes(info.fixedBytesEstimate), gigabytes(budget.bytes));
     }
-    // A resident feed to a progressive pipeline only addresses 50 slots.
-    if (info.needsWholeCloudResident && info.ringSlots == 0 && info.progressive &&
+    if (!g.fits) {
+        return format("refused: the budget is %.1f GB, below this pipeline's floor of %.1f GB (a %.1f GB %s, "
+                      "%.2f GB of fixed buffers and a %.2f GB smallest store); the whole cloud needs %.1f GB",
+                      gigabytes(budget.bytes), gigabytes(g.floor), gigabytes(g.feed), feedName,
+                      gigabytes(info.fixedBytesEstimate), gigabytes(info.minStoreBytes), gigabytes(g.need));
+    }
+    if (info.progressive && info.needsWholeCloudResident && info.ringSlots == 0 &&
         meta.numPoints > kMaxAddressablePoints) {
-        char buf[384];
-        std::snprintf(buf, sizeof(buf),
-                      "%s is configured for a resident cloud, and the builder addresses batch N at slot N %% %u, so "
-                      "a resident feed can only describe %.0fM points; this cloud has %.0fM. A streaming ring has "
-                      "no such limit.",
-                      info.displayName.c_str(), kBatchStreamSize, static_cast<double>(kMaxAddressablePoints) / 1e6,
+        return format("refused: %s keeps the cloud resident, but its builder finds batch b in slot b mod %u, so a "
+                      "resident feed reaches only the first %.0fM points of this %.0fM-point cloud; a streaming ring "
+                      "has no such ceiling",
+                      info.displayName.c_str(), kBatchStreamSize, kMaxAddressablePoints / 1e6,
                       static_cast<double>(meta.numPoints) / 1e6);
-        return buf;
     }
     return {};
 }
 
 bool PipelineRegistry::switchTo(const std::string& id, PointSource* source, const CloudMeta& meta,
                                 const DeviceBudget& budget, std::string* err) {
-    const Entry* entry = nullptr;
-    for (const Entry& e : m_entries)
-        if (e.info.id == id) entry = &e;
-    if (!entry) {
-        if (err) *err = "unknown pipeline: " + id;
+    auto fail = [&](const std::string& msg) {
+        if (err) *err = msg;
         return false;
-    }
-    const std::string reason = unsupportedReason(entry->info, meta, budget);
-    if (!reason.empty()) {
-        if (err) *err = entry->info.displayName + ": " + reason;
-        return false;
-    }
-    if (m_active) {
-        m_active->release();
-        m_active.reset();
-        m_activeId.clear();
-    }
-    // The feed's shape is the incoming pipeline's, decided before it allocates
-    // because the two share one budget.
+    };
+    const auto entry = std::find_if(m_entries.begin(), m_entries.end(), [&](const Entry& e) { return e.info.id == id; });
+    if (entry == m_entries.end()) return fail("unknown pipeline: " + id);
+    const std::string refusal = unsupportedReason(entry->info, meta, budget);
+    if (!refusal.empty()) return fail(entry->info.displayName + ": " + refusal);
+
+    // one pipeline holds device memory at a time: the old one goes first
+    shutdown();
     if (source) {
-        const PointSource::Mode mode =
-            entry->info.needsWholeCloudResident ? PointSource::Mode::Whole : PointSource::Mode::Stream;
-        if (!source->start(mode, entry->info.ringSlots, budget.bytes, err)) return false;
+        if (!source->start(feedMode(&entry->info), entry->info.ringSlots, budget.bytes, err)) return false;
         source->rewind();
     }
-    std::unique_ptr<ILodPipeline> pipeline = entry->factory();
-    if (!pipeline) {
-        if (err) *err = "factory returned null for " + id;
-        return false;
-    }
-    if (!pipeline->initPrograms(err)) return false;
-    if (!pipeline->allocate(meta, budget, err)) return false;
-    pipeline->reset();
-    m_active = std::move(pipeline);
+    std::unique_ptr<ILodPipeline> incoming = entry->factory();
+    if (!incoming) return fail("the factory of " + id + " made no pipeline");
+    if (!incoming->initPrograms(err) || !incoming->allocate(meta, budget, err)) return false;
+    incoming->reset();
+    m_active = std::move(incoming);
     m_activeId = id;
     return true;
 }
@@ -174,9 +208,7 @@ bool PipelineRegistry::reloadForCloud(PointSource* source, const CloudMeta& meta
     m_active->release();
     if (source) {
         const PipelineInfo* info = find(m_activeId);
-        const bool resident = !info || info->needsWholeCloudResident;
-        const PointSource::Mode mode = resident ? PointSource::Mode::Whole : PointSource::Mode::Stream;
-        if (!source->start(mode, info ? info->ringSlots : 0, budget.bytes, err)) return false;
+        if (!source->start(feedMode(info), info ? info->ringSlots : 0, budget.bytes, err)) return false;
         source->rewind();
     }
     if (!m_active->allocate(meta, budget, err)) return false;

@@ -51,7 +51,7 @@ public:
 
     bool start(Mode mode, uint32_t ringSlots, uint64_t maxDeviceBytes, std::string* err) override {
         if (m_meta.numPoints == 0) {
-            if (err) *err = "point cloud is empty";
+            if (err) *err = "the source holds no points";
             return false;
         }
         // Whole mode puts batch B at base + B * kSlotCapacity with no gaps, so the
@@ -59,7 +59,7 @@ public:
         const uint32_t batch = mode == Mode::Whole ? kSlotCapacity : m_batch;
         const uint32_t total = batchCount(m_meta.numPoints, batch);
         if (mode == Mode::Stream && ringSlots == 0) {
-            if (err) *err = "streaming ingest needs a ring depth; none was given";
+            if (err) *err = "Stream mode was asked for with a ring depth of 0 slots";
             return false;
         }
         const uint32_t slots = mode == Mode::Whole ? total : std::min(ringSlots, total);

@@ -110,3 +110,53 @@ def compare_accums(ctx, tree):
         assert list(g["c1"]) == list(a.c1), i
         assert list(g["c2"]) == list(a.c2), i
         assert g["count"] == a.count, i
+
+
+def quant28(coord, mn, size):
+    """The 28-bit octree coordinate of remolod_octree.cu:167-169 in IEEE float32
+    arithmetic (subtract, scale by 2^28 -- exact --, divide), converted with
+    saturating round-toward-zero as the CUDA path's __float2uint_rz."""
+    d = np.asarray(coord, dtype=np.float32) - np.float32(mn)
+    q = (np.float32(268435456.0) * d) / np.float32(size)
+    q = np.where(np.isnan(q) | (q < 0), np.float32(0), q).astype(np.float64)
+    return np.minimum(np.floor(q), 4294967295.0).astype(np.int64)
+
+
+def mix64(v):
+    v = np.asarray(v).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        v = (v ^ (v >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        v = (v ^ (v >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return v ^ (v >> np.uint64(31))
+
+
+def gpu_view(ctx):
+    """The GPU tree in the fixture format of tests/golden/make_ref_fixtures.py:
+    nodes keyed by (level, X, Y, Z) with order-independent digests of their
+    point multisets, voxel positions and occupancy grids."""
+    from test_ref_pin import grid_digest, multiset_digest
+    nodes = ctx.nodes()
+    keys = np.stack([nodes["level"], nodes["X"], nodes["Y"], nodes["Z"]], 1).astype(np.int64)
+    out = {"keys": keys, "counter": nodes["counter"].astype(np.int64),
+           "num_points": nodes["num_points"].astype(np.int64), "num_voxels": nodes["num_voxels"].astype(np.int64),
+           "is_leaf": nodes["is_leaf"].astype(bool), "has_grid": nodes["has_grid"].astype(bool)}
+    nn = len(nodes)
+    ckeys = np.full((nn, 8, 4), -1, dtype=np.int64)
+    for c in range(8):
+        m = nodes["child"][:, c] >= 0
+        ckeys[m, c] = keys[nodes["child"][m, c]]
+    out["child_keys"] = ckeys
+    pd = np.zeros(nn, dtype=np.uint64)
+    vd = np.zeros(nn, dtype=np.uint64)
+    gd = np.zeros(nn, dtype=np.uint64)
+    for i in range(nn):
+        if nodes["is_leaf"][i] and nodes["num_points"][i]:
+            p, _ = ctx.node_points(i)
+            pd[i] = multiset_digest(p.view(np.uint32).reshape(-1, 4))
+        if nodes["num_voxels"][i]:
+            v = ctx.node_voxels(i)
+            vd[i] = multiset_digest(v.view(np.uint32).reshape(-1, 4)[:, :3])
+        if nodes["has_grid"][i]:
+            gd[i] = grid_digest(ctx.node_grid(i))
+    out.update(point_digest=pd, voxel_digest=vd, grid_digest=gd)
+    return out

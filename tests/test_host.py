@@ -62,15 +62,21 @@ def test_gate_streaming_partial_tree(probe):
     assert probe[p + ".fits"] == "1"
     usable = (3_000_000_000 - RING_50 - REMOLOD_FIXED) - MARGIN
     assert abs(float(probe[p + ".predicted"]) - usable / 26 / 100_000_000) < 1e-8
-    assert probe[p + ".warning"].startswith("the budget holds about 54% of this cloud")
+    assert probe[p + ".warning"].startswith("predicted to take in about 54% of the cloud")
+    need_gb = (26 * 100_000_000 + RING_50 + REMOLOD_FIXED) / 1e9
+    assert f"needs a {need_gb:.1f} GB budget" in probe[p + ".warning"]
     assert probe[p + ".reason"] == ""
 
 
 def test_gate_refusal_below_floor(probe):
     p = "remolod_100M_1.9GB"
     assert probe[p + ".fits"] == "0"
-    assert probe[p + ".reason"].startswith("cannot run at all below 1.9 GB (0.8 GB ring + 0.59 GB fixed")
-    assert probe["switch_refused"].startswith("0 RemoLOD: cannot run at all below")
+    floor_gb = (MIN_STORE + RING_50 + REMOLOD_FIXED) / 1e9
+    reason = probe[p + ".reason"]
+    assert reason.startswith("refused: the budget is 1.9 GB, below this pipeline's floor of "
+                             f"{floor_gb:.1f} GB (a 0.8 GB ring, 0.59 GB of fixed buffers")
+    assert "smallest store" in reason
+    assert probe["switch_refused"].startswith("0 RemoLOD: refused: the budget is 0.0 GB")
 
 
 def test_gate_whole_fit_and_flat(probe):
@@ -79,7 +85,8 @@ def test_gate_whole_fit_and_flat(probe):
     # flat cannot truncate: its floor is the resident cloud itself
     assert int(probe["flat_100M_1.5GB.floor"]) == 16 * 100_000_000
     assert probe["flat_100M_1.5GB.fits"] == "0"
-    assert probe["flat_100M_1.5GB.reason"].startswith("needs 1.6 GB for 100000000 points and cannot build")
+    assert probe["flat_100M_1.5GB.reason"].startswith("refused: the whole cloud (100000000 points) needs 1.6 GB")
+    assert "cannot stop on a partial tree" in probe["flat_100M_1.5GB.reason"]
     assert probe["flat_100M_2GB.fits"] == "1"
     assert probe["flat_100M_2GB.predicted"] == "1.000000000"
 
@@ -93,7 +100,7 @@ def test_gate_small_cloud_prediction_kept(probe):
 
 
 def test_resident_ceiling(probe):
-    assert "can only describe 50M points; this cloud has 60M" in probe["resident_60M_100GB.reason"]
+    assert "reaches only the first 50M points of this 60M-point cloud" in probe["resident_60M_100GB.reason"]
     assert probe["resident_40M_100GB.reason"] == ""
 
 
@@ -219,4 +226,4 @@ def test_harness_refuses_small_budget(tmp_path, c1_cloud):
     rc, s, _, r = _run_harness(tmp_path, "--pipeline", "remolod", "--config", 1, "--seed", cfg.seed,
                                "--device-budget", 0.5, "--size", 64, 64)
     assert rc == 1
-    assert not s["ok"] and s["refused"].startswith("RemoLOD: cannot run at all below")
+    assert not s["ok"] and s["refused"].startswith("RemoLOD: refused: the budget is 0.5 GB")

@@ -70,6 +70,28 @@ def test_noalloc_render_matches_rb_render_twice_in_a_row(small_tree, edl):
         assert torch.equal(rgba, rgba_ref)
 
 
+def test_noalloc_render_takes_no_device_memory(small_tree):
+    """The claim itself: after one warm-up call (which only settles the
+    caching of torch's own tensors below), EDL-on renders leave the device's
+    free memory unchanged. rb_render would allocate its full-frame EDL copy the
+    first time it shades a frame this large; this entry point does not."""
+    import torch
+    from remobench_b200.lod import make_frame
+    ctx, bmin, bmax = small_tree
+    w, h = 1920, 1080
+    fb = torch.empty(w * h, dtype=torch.int64, device="cuda")
+    rgba = torch.empty(w * h, dtype=torch.int32, device="cuda")
+    f = make_frame(bmin, bmax, w, h, edl=True)
+    render_noalloc(ctx, f, fb, rgba)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for yaw in (0.3, 1.1, 2.0):
+        render_noalloc(ctx, make_frame(bmin, bmax, w, h, yaw=yaw, edl=True), fb, rgba)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_noalloc_rejects_contexts_beyond_its_limit():
     from remobench_b200 import synth
     from remobench_b200.lod import Context, make_frame

@@ -55,7 +55,9 @@ enum {
     RB_OVF_ARENA = 8u,     /* grid/chunk arena full */
     RB_OVF_TABLES = 64u,   /* chunk-table pool full */
     RB_OVF_DIRTY = 128u,   /* accumulate dirty list full */
-    RB_OVF_DRAWLIST = 256u /* render draw list full (remolod_render.cu:22) */
+    RB_OVF_DRAWLIST = 256u, /* render draw list full (remolod_render.cu:22) */
+    RB_OVF_SYNC = 512u      /* a device-side grid barrier gave up waiting: an error, the build
+                               call fails with RB_ERR_CUDA */
 };
 
 /* 16-byte point (include/remo/HostDeviceCommon.h:15-18): rgba with r in the low byte. */

@@ -28,7 +28,8 @@ enum KernelId : int {
     K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END, K_ACCUMULATE, K_ACCUM_VERIFY,
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
-    K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_SKIPPED, K_NUM
+    K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_PASS, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE,
+    K_EXPAND_REST, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
@@ -37,8 +38,8 @@ static const char* const kKernelNames[K_NUM] = {
     "k_frontier", "k_raster", "k_raster_flat", "k_edl", "k_resolve", "k_roll_level", "k_analyze",
     "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam",
     "k_expand_cond", "k_zero_grids",
-    // the four launches of an unrolled expand pass after the loop ended
-    "k_expand_skipped"};
+    // not a kernel: per-iteration expand passes run inside k_expand_rest
+    "expand_pass", "k_deep_book", "k_deep_bin", "k_deep_split", "k_deep_move", "k_expand_rest"};
 
 struct Profiler {
     bool on = false;
@@ -223,9 +224,12 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
     LAUNCH(c, K_BATCH_BEGIN, 1, rb::launchBatchBegin(d, s));
     LAUNCH(c, K_COUNT_FIRST, n, rb::launchCountFirst(d, pts, n, pointGrid(c, n), s));
     const int fixedGrid = c->numSMs * 4;
-    // the same kernels as the batch graph, with the loop test on the host;
-    // split and recount take their stamps from the device counters
-    LAUNCH(c, K_EXPAND_COND, 1, rb::launchExpandCond(d, s));
+    // the same kernels as the batch graph, with k_expand_rest's loop on the
+    // host; split and recount take their stamps from the device counters
+    LAUNCH(c, K_DEEP_BOOK, 1, rb::launchDeepBook(d, s));
+    LAUNCH(c, K_DEEP_BIN, n, rb::launchDeepBin(d, pts, n, pointGrid(c, n), s));
+    LAUNCH(c, K_DEEP_SPLIT, 1, rb::launchDeepSplit(d, s));
+    LAUNCH(c, K_DEEP_MOVE, n, rb::launchDeepMove(d, pts, n, pointGrid(c, n), s));
     for (uint32_t pass = 0; pass < 64u; pass++) {
         rb_status st = readCounters(c);
         if (st != RB_OK) return st;
@@ -233,7 +237,11 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
             *stopped = true;
             return RB_OK;
         }
-        if (c->hostCtr->numSpill == 0 || c->hostCtr->expandGuard > 40u) break;
+        // k_expand_rest's loop: a first pass if the round left spilling
+        // nodes, then more while the loop test says so
+        if (pass == 0 ? c->hostCtr->numSpill == 0 : c->hostCtr->loopMore == 0) break;
+        // the per-iteration passes k_expand_rest runs on the device
+        c->prof.launches[K_EXPAND_PASS] += 1;
         LAUNCH(c, K_SPLIT, c->hostCtr->numSpill, rb::launchSplit(d, 0u, s));
         LAUNCH(c, K_SPILL_COPY, 0, rb::launchSpillCopy(d, fixedGrid, s));
         LAUNCH(c, K_RECOUNT, n, rb::launchRecount(d, pts, n, 0u, pointGrid(c, n), s));
@@ -259,28 +267,33 @@ bool graphPath(rb_ctx* c) {
     if (!c->graphTried) {
         c->graphTried = true;
         const int pointGrid = c->numSMs * 8, fixedGrid = c->numSMs * 4;
-        if (rb::captureBatchGraph(c->d, pointGrid, fixedGrid, &c->batchGraph) != cudaSuccess) c->batchGraph = nullptr;
+        int restGrid = 0;
+        if (rb::expandRestGrid(c->numSMs, &restGrid) != cudaSuccess ||
+            rb::captureBatchGraph(c->d, pointGrid, fixedGrid, restGrid, &c->batchGraph) != cudaSuccess) {
+            cudaGetLastError();
+            c->batchGraph = nullptr;
+        }
     }
     return c->batchGraph != nullptr;
 }
 
-// Launches of graph batches, for the per-kernel counts: nine fixed kernels
-// and the loop test per batch, four kernels per expand pass, and four per
-// unrolled pass that ran after the loop ended (k_expand_skipped).
-void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint32_t skipsBefore, uint64_t points) {
-    // every batch graph runs the loop test once after its first count and once
-    // after each split pass; an unrolled pass after the loop ended launches its
-    // four kernels, which return at once
-    const uint32_t conds = c->hostCtr->condRuns - condBefore;
-    const uint32_t skips = c->hostCtr->condSkips - skipsBefore;
-    const uint64_t passes = conds >= batches ? conds - batches : 0u;
-    for (int k : {K_BATCH_BEGIN, K_COUNT_FIRST, K_ZERO_GRIDS, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS,
-                  K_INSERT, K_VOX_STORE, K_BATCH_END})
+// Launches of graph batches, for the per-kernel counts: fourteen kernels per
+// batch; the per-iteration passes k_expand_rest ran (one loop test each) are
+// counted as expand_pass, not as launches.
+void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint64_t points) {
+    const uint32_t passes = c->hostCtr->condRuns - condBefore;
+    for (int k : {K_BATCH_BEGIN, K_COUNT_FIRST, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE, K_EXPAND_REST,
+                  K_ZERO_GRIDS, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END})
         c->prof.launches[k] += batches;
-    c->prof.launches[K_EXPAND_COND] += conds;
-    for (int k : {K_SPLIT, K_SPILL_COPY, K_RECOUNT}) c->prof.launches[k] += passes;
-    c->prof.launches[K_EXPAND_SKIPPED] += 4ull * skips;
-    for (int k : {K_COUNT_FIRST, K_VOX_SAMPLE, K_INSERT}) c->prof.units[k] += points;
+    c->prof.launches[K_EXPAND_PASS] += passes;
+    for (int k : {K_COUNT_FIRST, K_DEEP_BIN, K_DEEP_MOVE, K_VOX_SAMPLE, K_INSERT}) c->prof.units[k] += points;
+}
+
+// A grid barrier of k_expand_rest gave up: the batch is not trustworthy.
+rb_status checkSync(rb_ctx* c) {
+    if (c->hostCtr->overflowFlags & rb::kOvfSync)
+        return fail(c, RB_ERR_CUDA, "a device grid barrier timed out in the expand passes (RB_OVF_SYNC)");
+    return RB_OK;
 }
 
 rb_status uploadRing(rb_ctx* c) {
@@ -561,6 +574,10 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.accumTo, N, "accumulate plan ranges");
     ALLOC(d.accumItem, (uint64_t)N + 1, "accumulate plan items");
     ALLOC(d.hist8, (uint64_t)N * 8, "child-octant counts");
+    ALLOC(d.deepCnt, (uint64_t)rb::kDeepRoots * rb::kDeepCells, "expand round bins");
+    ALLOC(d.deepSlot, N, "expand round root slots");
+    ALLOC(d.deepMeta, N, "expand round node codes");
+    ALLOC(d.deepPar, N / 8u + 1u, "expand round split lists");
     d.zeroCap = N / 8u + 1u;
     ALLOC(d.zeroList, d.zeroCap, "grids to zero");
     ALLOC(c->vis, N, "visible flags");
@@ -587,6 +604,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
 #undef ALLOC
     RB_CUDA(c, cudaMemsetAsync(d.hashSlots, 0xFF, (size_t)hashSize * 16, c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.ctr, 0, sizeof(Counters), c->stream));
+    RB_CUDA(c, cudaMemsetAsync(d.deepCnt, 0, (size_t)rb::kDeepRoots * rb::kDeepCells * 4, c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.accumGlobals, 0, sizeof(rb::AccumGlobals), c->stream));
     RB_CUDA(c, cudaMallocHost(&c->hostCtr, sizeof(Counters)));
     std::memset(c->hostCtr, 0, sizeof(Counters));
@@ -655,14 +673,15 @@ static rb_status buildFrom(rb_ctx* c, const rb::Point* ring, const uint32_t* siz
     uint32_t done = 0;
     bool stopped = false;
     if (graphs) {
-        const uint32_t condBefore = c->hostCtr->condRuns, skipsBefore = c->hostCtr->condSkips;
+        const uint32_t condBefore = c->hostCtr->condRuns;
         const uint64_t pointsBefore = c->hostCtr->numPointsProcessed;
         for (uint32_t k = 0; k < nb; k++) RB_CUDA(c, cudaGraphLaunch(c->batchGraph, c->stream));
         rb_status st = readCounters(c);
         if (st != RB_OK) return st;
+        if ((st = checkSync(c)) != RB_OK) return st;
         done = c->hostCtr->batchletIndex - first;
         stopped = c->hostCtr->batchStop && c->hostCtr->stopReason == rb::kStopMemory;
-        countGraphLaunches(c, nb, condBefore, skipsBefore, c->hostCtr->numPointsProcessed - pointsBefore);
+        countGraphLaunches(c, nb, condBefore, c->hostCtr->numPointsProcessed - pointsBefore);
         nb = 0;  // the batches ran on the device
     }
     for (uint32_t b = first; b < first + nb; b++) {
@@ -735,7 +754,7 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
     if ((uint64_t)firstBatch + nb > 0xFFFFFFFFull) return fail(c, RB_ERR_CAPACITY, "too many batches");
     const bool graphs = graphPath(c);
     uint64_t pointsBefore = 0;
-    uint32_t condBefore = 0, skipsBefore = 0;
+    uint32_t condBefore = 0;
     if (graphs) {
         rb::RingDesc& r = *c->hostRing;
         r.base = reinterpret_cast<unsigned long long>(c->ingestRing);
@@ -750,7 +769,6 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
         rb_status st = uploadRing(c);
         if (st != RB_OK) return st;
         condBefore = c->hostCtr->condRuns;
-        skipsBefore = c->hostCtr->condSkips;
         pointsBefore = c->hostCtr->numPointsProcessed;
     }
     RB_CUDA(c, cudaEventRecord(c->evStart, c->stream));
@@ -818,10 +836,11 @@ rb_status rb_ingest_host(rb_ctx* c, const rb_point* points, uint64_t n, uint32_t
     if (graphs) {
         rb_status st = readCounters(c);
         if (st != RB_OK) return st;
+        if ((st = checkSync(c)) != RB_OK) return st;
         c->batchesConsumed = c->hostCtr->batchletIndex;
         done = c->batchesConsumed - firstBatch;
         stopped = c->hostCtr->batchStop && c->hostCtr->stopReason == rb::kStopMemory;
-        countGraphLaunches(c, nb, condBefore, skipsBefore, c->hostCtr->numPointsProcessed - pointsBefore);
+        countGraphLaunches(c, nb, condBefore, c->hostCtr->numPointsProcessed - pointsBefore);
     }
     if (out) {
         float ms = 0.0f;

@@ -29,11 +29,20 @@ struct RenderScratch {
 // Update
 void launchBatchBegin(const Dev& d, cudaStream_t s);
 // One batch at the device cursor as an instantiated graph (see rb_update.cu).
-cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGraphExec_t* out);
+cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int restGrid, cudaGraphExec_t* out);
+// The cooperative expand-pass kernel: its grid, and one launch.
+cudaError_t expandRestGrid(int numSMs, int* grid);
+cudaError_t launchExpandRest(const Dev& d, int grid, cudaStream_t s);
 void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchRecount(const Dev& d, const Point* pts, uint32_t n, uint32_t prevStamp, int grid, cudaStream_t s);
 void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s);
 void launchZeroGrids(const Dev& d, int grid, cudaStream_t s);
+// the expand round (rb_update.cu): book the first count's splits, bin the
+// points below them, make every split the counts decide, move the points
+void launchDeepBook(const Dev& d, cudaStream_t s);
+void launchDeepBin(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
+void launchDeepSplit(const Dev& d, cudaStream_t s);
+void launchDeepMove(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchExpandCond(const Dev& d, cudaStream_t s);
 void launchSpillCopy(const Dev& d, int grid, cudaStream_t s);
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);

@@ -84,6 +84,16 @@ struct Counters {
     uint32_t histValid;           // hist8 holds the child-octant counts of the nodes to split next
     uint32_t countLo, countHi;    // nodes [countLo, countHi) whose points the next recount counts
     uint32_t condRuns;            // runs of the expand loop's test since allocation (wraps)
+    // the batch's multi-level expand round (rb_update.cu, k_deep_*): active
+    // when its roots (the first count's spilling nodes) were booked
+    uint32_t deepActive;
+    uint32_t deepRoots;           // roots booked, in increasing id (slot order)
+    uint32_t deepLevels;          // levels below the roots whose counts are binned
+    uint32_t deepBase;            // id of the roots' first child
+    uint32_t deepStamp;           // split stamp of the roots
+    // grid barrier of the cooperative expand kernel (k_expand_rest), per batch
+    uint32_t barArrive;
+    uint32_t barRelease;
 };
 
 enum StopReason : uint32_t { kStopMemory = 1u, kStopNoBatch = 2u, kStopTime = 3u };
@@ -114,6 +124,7 @@ enum OverflowBits : uint32_t {
     kOvfTables = 64u,     // chunk-table pool full
     kOvfDirty = 128u,     // dirty list full
     kOvfDrawList = 256u,  // render draw list full
+    kOvfSync = 512u,      // a grid barrier gave up waiting (an error, not a capacity)
 };
 
 // One node split by the last split pass: where its stored points go.
@@ -219,6 +230,14 @@ struct Dev {
     // per node, its points per child octant, counted by the recount for the
     // nodes made by the last split: one level of lookahead for the next split
     uint32_t* hist8;         // [maxNodes * 8]
+    // multi-level expand round: per root slot, the points below it counted at
+    // every depth 1..kDeepLevels ([kDeepRoots][kDeepCells]); per root node its
+    // slot; per node made by the round, (slot << 16) | its code below the root;
+    // per generation, the nodes split in id order
+    uint32_t* deepCnt;
+    uint32_t* deepSlot;      // [maxNodes]
+    uint32_t* deepMeta;      // [maxNodes]
+    uint32_t* deepPar;       // [maxNodes / 8 + 1]
     uint32_t zeroCap;
     // capacities and constants
     uint32_t maxNodes;
@@ -242,6 +261,14 @@ struct Dev {
 };
 
 constexpr uint32_t kGridUnits = (uint32_t)(kGridBytes / 16u);
+
+// The multi-level expand round bins the points below each of up to kDeepRoots
+// spilling nodes at depths 1..kDeepLevels below it: depth j has 8^j cells,
+// stored from deepOffset(j), kDeepCells per root in all.
+constexpr uint32_t kDeepLevels = 4;
+constexpr uint32_t kDeepRoots = 512;
+__host__ __device__ constexpr uint32_t deepOffset(uint32_t depth) { return ((1u << (3u * depth)) - 8u) / 7u; }
+constexpr uint32_t kDeepCells = deepOffset(kDeepLevels + 1u);
 
 #ifdef __CUDACC__
 __device__ __forceinline__ Point* chunkPoints(const Dev& d, uint32_t phys) {

@@ -241,6 +241,10 @@ __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     c->countLo = 0;
     c->countHi = 0;
     c->hashNeedsClear = 0;  // the last batch's k_vox_store emptied the table
+    c->deepActive = 0;
+    c->deepRoots = 0;
+    c->barArrive = 0;
+    c->barRelease = 0;
 }
 
 // Iteration 1 of expand (doCounting over the batch, remolod_octree.cu:225-229):
@@ -294,8 +298,8 @@ __global__ void __launch_bounds__(256) k_count_first(Dev d, const Point* __restr
 //
 // prevStamp == 0: device-driven; the stamp of the last split's first round,
 // and no recount once the pass limit is reached.
-__global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict__ pts, uint32_t n,
-                                                 uint32_t prevStamp, uint32_t gated) {
+__device__ __forceinline__ void recountBody(const Dev& d, const Point* __restrict__ pts, uint32_t n,
+                                            uint32_t prevStamp, uint32_t gated) {
     Counters* c = d.ctr;
     if (c->batchStop || (gated && c->loopMore == 0u)) return;
     if (prevStamp == 0u) {
@@ -341,6 +345,11 @@ __global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict_
     blockCountsFlush<true>(d, s_counts);
 }
 
+__global__ void __launch_bounds__(256) k_recount(Dev d, const Point* __restrict__ pts, uint32_t n,
+                                                 uint32_t prevStamp, uint32_t gated) {
+    recountBody(d, pts, n, prevStamp, gated);
+}
+
 // Block-wide exclusive scan of one value per thread (blockDim.x == 1024).
 __device__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* total, uint32_t* s_warp) {
     const uint32_t lane = laneId(), warp = threadIdx.x >> 5;
@@ -375,7 +384,7 @@ __device__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* total, uint32_t* s_
 // Device-driven builds (h != 0) set the loop's condition: another pass while
 // nodes spill, at most 40 passes (max_expand_iters <= 31 are needed).
 // One block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_expand_cond(Dev d, cudaGraphConditionalHandle h, uint32_t gated) {
+__device__ __forceinline__ void expandCondBody(const Dev& d, cudaGraphConditionalHandle h, uint32_t gated) {
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_run;
     Counters* c = d.ctr;
@@ -429,6 +438,10 @@ __global__ void __launch_bounds__(1024) k_expand_cond(Dev d, cudaGraphConditiona
         c->loopMore = more ? 1u : 0u;
         if (h != 0ull) cudaGraphSetConditional(h, more ? 1u : 0u);
     }
+}
+
+__global__ void __launch_bounds__(1024) k_expand_cond(Dev d, cudaGraphConditionalHandle h, uint32_t gated) {
+    expandCondBody(d, h, gated);
 }
 
 // Ascending bitonic sort of n ids in place (single block); pads with kNone.
@@ -538,7 +551,7 @@ __device__ __forceinline__ void splitBook(const Dev& d, Counters* c, uint32_t k,
 // the reference's 36M cloud, wiki/03_ExpandStageFindings.md:63) are sorted,
 // scanned and booked by one warp with no block barrier; more go through a
 // block-wide sort and scans.
-__global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp, uint32_t gated) {
+__device__ __forceinline__ void splitBody(const Dev& d, uint32_t stamp, uint32_t gated) {
     __shared__ uint32_t s_sort[kSortSmem];
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_runPts, s_runChunks, s_acc, s_nn, s_run2;
@@ -821,10 +834,12 @@ __global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp, uint32_t 
     }
 }
 
+__global__ void __launch_bounds__(1024) k_split(Dev d, uint32_t stamp, uint32_t gated) { splitBody(d, stamp, gated); }
+
 // The split nodes' stored points move to the spill list (remolod_octree.cu:250-285)
 // and their chunks return to the queue (:349-360): one work item per owned
 // chunk, strided over blocks.
-__global__ void __launch_bounds__(256) k_spill_copy(Dev d, uint32_t gated) {
+__device__ __forceinline__ void spillCopyBody(const Dev& d, uint32_t gated) {
     const Counters* c = d.ctr;
     if (c->batchStop || (gated && c->loopMore == 0u)) return;
     const uint32_t nsplit = c->numSplit;
@@ -857,16 +872,463 @@ __global__ void __launch_bounds__(256) k_spill_copy(Dev d, uint32_t gated) {
     }
 }
 
-// The grids of the nodes split in this batch, zeroed (:372-387) once after
-// the expand loop: one block per grid.
+__global__ void __launch_bounds__(256) k_spill_copy(Dev d, uint32_t gated) { spillCopyBody(d, gated); }
+
+// ------------------------------------------------------------ expand round
+//
+// The reference's expand loop (remolod_octree.cu:402-462) counts, splits the
+// nodes over the limit, moves their points one level down and counts again,
+// up to 20 times per batch. The nodes a batch splits are decided by its first
+// count alone: iteration 1 lists the spilling leaves (the roots), and every
+// later iteration counts only nodes made by the previous split, i.e. the cubes
+// below the roots. So one pass that bins every point below a root by its cube
+// at depths 1..kDeepLevels gives every count those iterations would take, and
+// the splits, the ids they hand out and every counter follow from the counts
+// in the reference's order: iteration by iteration, the spilling nodes in
+// increasing id, each taking the next 8 ids. A round is four kernels --
+// k_deep_book (book the roots' splits), k_deep_bin (spill their stored points
+// and bin every point below a root), k_deep_split (all splits of iterations
+// 1 .. 1 + kDeepLevels - 1) and k_deep_move (every moved point to its final
+// leaf) -- instead of a count, split and recount per iteration. Cubes still
+// over the limit at depth kDeepLevels (rare: 50,000 points in 1/4096 of a
+// spilling node) go on through the per-iteration passes, as do batches whose
+// first count lists more than kDeepRoots nodes or a node at the deepest level.
+
+// A new node: child `i` of `parent` at id `ch` (doSplitting's child set-up,
+// remolod_octree.cu:323-347), with its ancestor row.
+__device__ __forceinline__ void makeChild(const Dev& d, uint32_t ch, uint32_t parent, uint32_t i) {
+    const uint32_t plv = d.level[parent], pg = d.grid[parent];
+    const uint32_t lv = plv + 1u;
+#pragma unroll
+    for (int q = 0; q < 8; q++) d.child[ch * 8u + q] = -1;
+    d.counter[ch] = 0;
+    reinterpret_cast<uint4*>(d.hist8 + (size_t)ch * 8u)[0] = make_uint4(0, 0, 0, 0);
+    reinterpret_cast<uint4*>(d.hist8 + (size_t)ch * 8u)[1] = make_uint4(0, 0, 0, 0);
+    d.numPoints[ch] = 0;
+    d.level[ch] = lv;
+    d.nodeX[ch] = 2u * d.nodeX[parent] + ((i >> 2) & 1u);
+    d.nodeY[ch] = 2u * d.nodeY[parent] + ((i >> 1) & 1u);
+    d.nodeZ[ch] = 2u * d.nodeZ[parent] + (i & 1u);
+    d.grid[ch] = kNone;
+    d.numVoxels[ch] = 0;
+    d.numVoxelsStored[ch] = 0;
+    d.numPointChunks[ch] = 0;
+    d.numVoxelChunks[ch] = 0;
+    d.ptTableOff[ch] = kNone;
+    d.ptTableCap[ch] = 0;
+    d.vxTableOff[ch] = kNone;
+    d.vxTableCap[ch] = 0;
+    d.splitIter[ch] = 0;
+    d.dirtyStamp[ch] = 0;
+    AccumI z = {};
+    d.accum[ch] = z;
+    const uint2* prow = d.anc + (size_t)parent * kMaxDepth;
+    uint2* crow = d.anc + (size_t)ch * kMaxDepth;
+#pragma unroll
+    for (uint32_t l = 0; l < (uint32_t)kMaxDepth; l++)
+        if (l + 1u < lv) crow[l] = prow[l];
+    crow[lv - 1u] = make_uint2(parent, pg);
+    d.child[parent * 8u + i] = (int32_t)ch;
+}
+
+// The bookkeeping every split shares: a grid if the node has none (allocated
+// once, zeroed at every split, :365-387), its split stamp, the grid on the
+// zero list and the node on the dirty list.
+__device__ __forceinline__ void bookSplit(const Dev& d, Counters* c, uint32_t node, uint32_t stamp) {
+    uint32_t g = d.grid[node];
+    if (g == kNone) {
+        g = arenaAlloc(d, kGridUnits);
+        d.grid[node] = g;
+        atomicAdd(&c->numGrids, 1u);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset), (unsigned long long)refAllocSize(kGridBytes));
+    }
+    d.splitIter[node] = stamp;
+    if (g != kNone) {
+        const uint32_t z = atomicAdd(&c->numZero, 1u);
+        if (z < d.zeroCap) d.zeroList[z] = g;
+    }
+    if (d.dirtyStamp[node] != c->buildStamp) {
+        d.dirtyStamp[node] = c->buildStamp;
+        const uint32_t di = atomicAdd(&c->numDirty, 1u);
+        if (di < d.maxNodes) d.dirtyList[di] = node;
+    }
+}
+
+// Iteration 1's splits (doSplitting for the first count's spilling nodes, in
+// increasing id): their bookkeeping, where their stored points go in the
+// spill list, their chunks' queue positions. The children are made by
+// k_deep_split with the later generations. One block of 1024 threads. Leaves
+// the round off (the per-iteration passes take the batch) when no node can
+// be split, more than kDeepRoots spill, or a root lies too deep to bin below.
+__global__ void __launch_bounds__(1024) k_deep_book(Dev d) {
+    __shared__ uint32_t s_sort[kDeepRoots];
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_maxLevel;
+    Counters* c = d.ctr;
+    if (c->batchStop) return;
+    uint32_t ns = c->numSpill;
+    if (ns > d.spillingCap) ns = d.spillingCap;
+    if (ns == 0u || ns > kDeepRoots) return;
+    const uint32_t n0 = c->numNodes;
+    const uint32_t room = d.maxNodes > n0 ? (d.maxNodes - n0) / 8u : 0u;
+    const uint32_t acc = ns < room ? ns : room;
+    if (acc == 0u) return;
+    for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s_sort[i] = d.spillNodes[i];
+    if (threadIdx.x == 0) s_maxLevel = 0;
+    __syncthreads();
+    bitonicSort(s_sort, ns);
+    for (uint32_t k = threadIdx.x; k < acc; k += blockDim.x) atomicMax(&s_maxLevel, d.level[s_sort[k]]);
+    __syncthreads();
+    const uint32_t maxLevel = s_maxLevel;
+    if (maxLevel >= (uint32_t)kMaxDepth) return;
+    const uint32_t depthRoom = (uint32_t)kMaxDepth - maxLevel;
+    const uint32_t levels = depthRoom < kDeepLevels ? depthRoom : kDeepLevels;
+    const uint32_t it0 = c->iter;
+    const uint32_t stamp = (c->batchletIndex << 5) | it0;
+    const uint32_t spilledBefore = c->numSpilled;
+    // acc <= kDeepRoots < blockDim.x: one scan covers every root
+    const uint32_t k = threadIdx.x;
+    uint32_t node = 0, np = 0, owned = 0;
+    if (k < acc) {
+        node = s_sort[k];
+        owned = d.numPointChunks[node];
+        const uint32_t cap = owned * d.ppc;
+        np = d.numPoints[node] < cap ? d.numPoints[node] : cap;
+    }
+    uint32_t totPts, totCh;
+    const uint32_t prePts = blockExclusiveScan(np, &totPts, s_warp);
+    const uint32_t preCh = blockExclusiveScan(owned, &totCh, s_warp);
+    if (k < acc) {
+        bookSplit(d, c, node, stamp);
+        SplitRec r;
+        r.node = node;
+        r.numPoints = np;
+        r.tableOff = d.ptTableOff[node];
+        r.spillBase = spilledBefore + prePts;
+        r.chunkBase = preCh;
+        r.numChunks = owned;
+        r.grid = d.grid[node];
+        // the node's chunks go back to the queue (remolod_octree.cu:349-360)
+        r.queueBase = owned ? atomicSub(&c->numAllocatedChunks, owned) - owned : kNone;
+        d.splitRecs[k] = r;
+        d.numPoints[node] = 0;
+        d.numPointChunks[node] = 0;
+        d.ptTableOff[node] = kNone;
+        d.ptTableCap[node] = 0;
+        d.deepSlot[node] = k;
+    }
+    if (threadIdx.x == 0) {
+        if (acc < ns) c->nodePoolOverflow = 1;
+        uint32_t total = spilledBefore + totPts;
+        if (total > d.spillCap) {
+            atomicOr(&c->overflowFlags, (uint32_t)kOvfSpilled);
+            total = d.spillCap;
+        }
+        c->numSpilled = total;
+        c->numSplit = acc;
+        c->spillChunkTotal = totCh;
+        c->nodesSplit += acc;
+        c->numSpill = 0;
+        c->lastStamp = stamp;
+        c->histValid = 0;
+        c->countLo = 0;
+        c->countHi = 0;
+        c->deepRoots = acc;
+        c->deepLevels = levels;
+        c->deepBase = n0;
+        c->deepStamp = stamp;
+        c->deepActive = 1;
+    }
+}
+
+// One point below root slot `slot` (at level lv) into its cubes at depths
+// 1..levels. Every lane of the warp calls it; lanes with no point pass
+// active = false. Equal cubes in a warp add once.
+__device__ __forceinline__ void deepBin(const Dev& d, bool active, uint32_t slot, uint32_t lv, const Point& p,
+                                        uint32_t levels) {
+    uint32_t x = 0, y = 0, z = 0;
+    if (active) {
+        x = quant20(p.x, d.boxMin[0], d.octreeSize);
+        y = quant20(p.y, d.boxMin[1], d.octreeSize);
+        z = quant20(p.z, d.boxMin[2], d.octreeSize);
+    }
+    uint32_t code = 0;
+#pragma unroll
+    for (uint32_t j = 1; j <= kDeepLevels; j++) {
+        if (j > levels) break;  // the same for every lane
+        code = (code << 3) | (active ? childIndex(x, y, z, lv + j - 1u) : 0u);
+        const uint32_t key = active ? slot * kDeepCells + deepOffset(j) + code : kNone;
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+        if (active && (int)laneId() == __ffs(peers) - 1) atomicAdd(&d.deepCnt[key], (uint32_t)__popc(peers));
+    }
+}
+
+// The roots' stored points move to the spill list (remolod_octree.cu:250-285)
+// and their chunks return to the queue (:349-360), one work item per owned
+// chunk; then every batch point whose leaf is a root. Each is binned below its
+// root.
+__global__ void __launch_bounds__(256) k_deep_bin(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    const Counters* c = d.ctr;
+    if (c->batchStop || !c->deepActive) return;
+    RB_BATCH_AT_CURSOR(d, pts, n);
+    const uint32_t levels = c->deepLevels, stamp = c->deepStamp;
+    const uint32_t nsplit = c->numSplit, nchunk = c->spillChunkTotal;
+    for (uint32_t w = blockIdx.x; w < nchunk; w += gridDim.x) {
+        uint32_t lo = 0, hi = nsplit;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (d.splitRecs[mid].chunkBase <= w) lo = mid;
+            else hi = mid;
+        }
+        const SplitRec r = d.splitRecs[lo];
+        const uint32_t j = w - r.chunkBase;
+        const uint32_t phys = d.tablePool[r.tableOff + j];
+        if (threadIdx.x == 0 && r.queueBase + j < d.maxPtChunks) d.chunkQueue[r.queueBase + j] = phys;
+        if (phys == kNone) continue;
+        const uint32_t lv = d.level[r.node];
+        const uint32_t first = j * d.ppc;
+        const uint32_t last = first + d.ppc < r.numPoints ? first + d.ppc : r.numPoints;
+        for (uint32_t b = first; b < last; b += blockDim.x) {
+            const uint32_t s = b + threadIdx.x;
+            const uint32_t slot = r.spillBase + s;
+            const bool active = s < last && slot < d.spillCap;
+            Point q = {0.f, 0.f, 0.f, 0u};
+            if (active) {
+                q = chunkPoints(d, phys)[s - first];
+                d.spillPts[slot] = q;
+                d.spillIdx[slot] = chunkIndices(d, phys)[s - first];
+                d.spillLeaf[slot] = r.node;
+            }
+            deepBin(d, active, lo, lv, q, levels);
+        }
+    }
+    for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
+        const uint32_t i = b + threadIdx.x;
+        uint32_t leaf = 0;
+        bool active = false;
+        if (i < n) {
+            leaf = d.leafOf[i];
+            active = d.splitIter[leaf] == stamp;
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) continue;
+        Point p = {0.f, 0.f, 0.f, 0u};
+        uint32_t slot = 0, lv = 0;
+        if (active) {
+            p = loadPoint(pts + i);
+            slot = d.deepSlot[leaf];
+            lv = d.level[leaf];
+        }
+        deepBin(d, active, slot, lv, p, levels);
+    }
+}
+
+// Iterations 2 .. 1 + kDeepLevels from the binned counts: generation g (the
+// nodes made by iteration g's splits, g >= 1) is counted in iteration g + 1;
+// its nodes over the limit split in that iteration, in increasing id, each
+// taking the next 8 ids (the pool guard refuses them once fewer than 8 ids
+// remain, :318-321), and the loop ends at the first iteration that splits
+// nothing or at the pass limit. Nodes of the last generation counted and
+// still over the limit are handed to the per-iteration passes. One block of
+// 1024 threads.
+__global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_acc, s_cont;
+    Counters* c = d.ctr;
+    if (c->batchStop || !c->deepActive) return;
+    const uint32_t roots = c->deepRoots, levels = c->deepLevels, base = c->deepBase, it0 = c->iter;
+    const uint32_t batchTag = c->batchletIndex << 5;
+    // generation 1: the roots' children, 8 consecutive ids per root in slot order
+    for (uint32_t t = threadIdx.x; t < 8u * roots; t += blockDim.x) {
+        makeChild(d, base + t, d.splitRecs[t >> 3].node, t & 7u);
+        d.deepMeta[t] = ((t >> 3) << 16) | (t & 7u);
+    }
+    uint32_t lo = base, hi = base + 8u * roots;
+    uint32_t splits = 0, itEnd = 0, cont = 0;
+    for (uint32_t g = 1;; g++) {
+        const uint32_t it = it0 + g;  // the iteration that counts generation g
+        if (it > d.maxExpandIters) {
+            itEnd = it;  // the loop ended after the split that made generation g
+            break;
+        }
+        const uint32_t room = d.maxNodes > hi ? (d.maxNodes - hi) / 8u : 0u;
+        if (threadIdx.x == 0) {
+            s_acc = 0;
+            s_cont = 0;
+        }
+        __syncthreads();
+        for (uint32_t t0 = lo; t0 < hi; t0 += blockDim.x) {
+            const uint32_t node = t0 + threadIdx.x;
+            uint32_t cnt = 0;
+            if (node < hi) {
+                const uint32_t meta = d.deepMeta[node - base];
+                cnt = d.deepCnt[(meta >> 16) * kDeepCells + deepOffset(g) + (meta & 0xFFFFu)];
+                d.counter[node] = cnt;
+            }
+            const bool over = node < hi && cnt > d.maxPointsPerNode;
+            const uint32_t wantSplit = (over && g < levels) ? 1u : 0u;
+            const uint32_t wantCont = (over && g == levels) ? 1u : 0u;
+            uint32_t totS, totC;
+            const uint32_t preS = blockExclusiveScan(wantSplit, &totS, s_warp);
+            const uint32_t preC = blockExclusiveScan(wantCont, &totC, s_warp);
+            const uint32_t j = s_acc + preS;
+            if (wantSplit && j < room) {
+                bookSplit(d, c, node, batchTag | it);
+                d.deepPar[j] = node;
+            }
+            const uint32_t jc = s_cont + preC;
+            if (wantCont && jc < d.spillingCap) d.spillNodes[jc] = node;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_acc += totS;
+                s_cont += totC;
+            }
+            __syncthreads();
+        }
+        const uint32_t want = s_acc;
+        const uint32_t nacc = want < room ? want : room;
+        if (threadIdx.x == 0 && nacc < want) c->nodePoolOverflow = 1;
+        if (nacc == 0u) {
+            cont = s_cont;
+            // continuation: the per-iteration passes split them in this
+            // iteration; every spiller refused: one more, empty, count
+            itEnd = cont > 0u ? it : (want > 0u ? it + 1u : it);
+            break;
+        }
+        splits += nacc;
+        // the children of this iteration's splits, ids [hi, hi + 8 nacc)
+        for (uint32_t t = threadIdx.x; t < 8u * nacc; t += blockDim.x) {
+            const uint32_t parent = d.deepPar[t >> 3];
+            const uint32_t pm = d.deepMeta[parent - base];
+            makeChild(d, hi + t, parent, t & 7u);
+            d.deepMeta[hi + t - base] = (pm & 0xFFFF0000u) | (((pm & 0xFFFFu) << 3) | (t & 7u));
+        }
+        __syncthreads();
+        lo = hi;
+        hi += 8u * nacc;
+    }
+    if (threadIdx.x == 0) {
+        c->numNodes = hi;
+        c->nodesSplit += splits;
+        c->iter = itEnd;
+        if (cont > d.spillingCap) {
+            atomicOr(&c->overflowFlags, (uint32_t)kOvfSpilling);
+            cont = d.spillingCap;
+        }
+        c->numSpill = cont;
+    }
+}
+
+// Every point the round moved -- batch points and spilled points whose leaf
+// is a root -- down the finished subtree to its leaf.
+__global__ void __launch_bounds__(256) k_deep_move(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    const Counters* c = d.ctr;
+    if (c->batchStop || !c->deepActive) return;
+    RB_BATCH_AT_CURSOR(d, pts, n);
+    const uint32_t stamp = c->deepStamp;
+    const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
+    const uint32_t total = n + ns;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const bool batchPt = i < n;
+        uint32_t cur = batchPt ? d.leafOf[i] : d.spillLeaf[i - n];
+        if (d.splitIter[cur] != stamp) continue;
+        const Point p = batchPt ? loadPoint(pts + i) : d.spillPts[i - n];
+        const uint32_t x = quant20(p.x, d.boxMin[0], d.octreeSize), y = quant20(p.y, d.boxMin[1], d.octreeSize),
+                       z = quant20(p.z, d.boxMin[2], d.octreeSize);
+        uint32_t lv = d.level[cur];
+        while (lv < (uint32_t)kMaxDepth) {
+            const int32_t nx = d.child[cur * 8u + childIndex(x, y, z, lv)];
+            if (nx < 0) break;
+            cur = (uint32_t)nx;
+            lv += 1u;
+        }
+        if (batchPt) d.leafOf[i] = cur;
+        else d.spillLeaf[i - n] = cur;
+    }
+}
+
+// Grid-wide barrier of a cooperative launch. Every block is resident, so the
+// wait ends once each block arrives; the polls are still bounded (about a
+// second), after which the block records kOvfSync, the others stop waiting
+// when they see it, and the caller returns. Thread 0 of each block keeps the
+// barrier's epoch count.
+__device__ bool gridBarrier(Counters* c, uint32_t& epoch) {
+    __shared__ uint32_t s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        epoch += 1u;
+        uint32_t ok = 1;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(&c->barArrive, 1u) + 1u;
+        if (arrived == epoch * gridDim.x) {
+            __threadfence();
+            atomicExch(&c->barRelease, epoch);
+        } else {
+            const volatile uint32_t* rel = &c->barRelease;
+            const volatile uint32_t* flags = &c->overflowFlags;
+            for (uint32_t spins = 0; *rel < epoch; spins++) {
+                if (spins > (1u << 24) || (*flags & kOvfSync)) {
+                    atomicOr(&c->overflowFlags, (uint32_t)kOvfSync);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0u;
+}
+
+// The per-iteration passes (split, spill copy, recount, loop test) for a
+// batch the expand round left unfinished -- nodes still over the limit at its
+// deepest binned level, or a first count it did not take -- as one
+// cooperative kernel with grid barriers between the phases, so the batch
+// graph needs no conditional node. Most batches return at once: the round
+// left nothing to split. Launched with one 1024-thread block per SM.
+__global__ void __launch_bounds__(1024, 1) k_expand_rest(Dev d) {
+    Counters* c = d.ctr;
+    // no block writes these before the first barrier: every block decides alike
+    if (c->batchStop || c->numSpill == 0u) return;
+    uint32_t epoch = 0;
+    for (uint32_t pass = 0; pass < 64u; pass++) {
+        if (!gridBarrier(c, epoch)) return;
+        if (blockIdx.x == 0) splitBody(d, 0u, 0u);
+        if (!gridBarrier(c, epoch)) return;
+        spillCopyBody(d, 0u);
+        if (!gridBarrier(c, epoch)) return;
+        recountBody(d, nullptr, 0u, 0u, 0u);
+        if (!gridBarrier(c, epoch)) return;
+        if (blockIdx.x == 0) expandCondBody(d, 0ull, 0u);
+        if (!gridBarrier(c, epoch)) return;
+        // the next pass's split comes after its first barrier: all read alike
+        if (c->loopMore == 0u) return;
+    }
+}
+
+// The grids of the nodes split in this batch (zeroed at every split,
+// :372-387) and the expand round's bins, cleared once after the expand loop
+// (nothing reads a split grid before voxel sampling). Work items of 16 KB
+// spread over every block.
 __global__ void __launch_bounds__(256) k_zero_grids(Dev d) {
     const Counters* c = d.ctr;
     if (c->batchStop) return;
     const uint32_t nz = c->numZero < d.zeroCap ? c->numZero : d.zeroCap;
+    constexpr uint32_t kPiece = 1024;  // uint4 per work item
+    constexpr uint32_t kPieces = kGridWords / 4u / kPiece;
+    const uint32_t deepUnits = (c->deepRoots * kDeepCells + 3u) / 4u;  // rows are contiguous from slot 0
+    const uint32_t deepItems = (deepUnits + kPiece - 1u) / kPiece;
     const uint4 z = make_uint4(0, 0, 0, 0);
-    for (uint32_t w = blockIdx.x; w < nz; w += gridDim.x) {
-        uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, d.zeroList[w]));
-        for (uint32_t q = threadIdx.x; q < kGridWords / 4u; q += blockDim.x) g[q] = z;
+    for (uint32_t w = blockIdx.x; w < nz * kPieces + deepItems; w += gridDim.x) {
+        if (w < nz * kPieces) {
+            uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, d.zeroList[w / kPieces])) + (w % kPieces) * kPiece;
+            for (uint32_t q = threadIdx.x; q < kPiece; q += blockDim.x) g[q] = z;
+        } else {
+            const uint32_t u0 = (w - nz * kPieces) * kPiece;
+            uint4* g = reinterpret_cast<uint4*>(d.deepCnt);
+            for (uint32_t q = u0 + threadIdx.x; q < u0 + kPiece && q < deepUnits; q += blockDim.x) g[q] = z;
+        }
     }
 }
 
@@ -1545,6 +2007,37 @@ void launchSplit(const Dev& d, uint32_t stamp, cudaStream_t s) { k_split<<<1, 10
 void launchExpandCond(const Dev& d, cudaStream_t s) { k_expand_cond<<<1, 1024, 0, s>>>(d, 0ull, 0u); }
 void launchSpillCopy(const Dev& d, int grid, cudaStream_t s) { k_spill_copy<<<grid, 256, 0, s>>>(d, 0u); }
 void launchZeroGrids(const Dev& d, int grid, cudaStream_t s) { k_zero_grids<<<grid, 256, 0, s>>>(d); }
+void launchDeepBook(const Dev& d, cudaStream_t s) { k_deep_book<<<1, 1024, 0, s>>>(d); }
+void launchDeepBin(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
+    k_deep_bin<<<grid, 256, 0, s>>>(d, pts, n);
+}
+void launchDeepSplit(const Dev& d, cudaStream_t s) { k_deep_split<<<1, 1024, 0, s>>>(d); }
+void launchDeepMove(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
+    k_deep_move<<<grid, 256, 0, s>>>(d, pts, n);
+}
+
+// k_expand_rest's cooperative grid: every block resident at once.
+cudaError_t expandRestGrid(int numSMs, int* grid) {
+    int perSM = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_expand_rest, 1024, 0);
+    if (e != cudaSuccess) return e;
+    if (perSM < 1) return cudaErrorCooperativeLaunchTooLarge;
+    *grid = numSMs;  // one block per SM is all the passes need
+    return cudaSuccess;
+}
+
+cudaError_t launchExpandRest(const Dev& d, int grid, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(1024);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_expand_rest, d);
+}
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_vox_sample<<<grid, 256, 0, s>>>(d, pts, n);
 }
@@ -1558,67 +2051,28 @@ void launchBatchEnd(const Dev& d, uint32_t n, cudaStream_t s) { k_batch_end<<<1,
 void launchSweep(const Dev& d, int grid, cudaStream_t s) { k_sweep<<<grid, 256, 0, s>>>(d); }
 void launchResetRoot(const Dev& d, int grid, cudaStream_t s) { k_reset_root<<<grid, 256, 0, s>>>(d); }
 
-// One batch as a CUDA graph: the phase kernels of runBatch with the expand
-// loop as a conditional WHILE node, every kernel reading its batch from the
-// device cursor. One graph launch builds the batch at batchletIndex with no
-// host round trip; a stopped batch (memory, no batch uploaded, time budget)
-// runs through as no-ops.
-// Expand passes captured as plain kernels ahead of the loop node: a pass after
-// the loop ended costs four launches that return at once, while entering and
-// leaving a conditional node's body costs several microseconds per pass and
-// per batch. Batches that need more passes finish in the loop node.
-constexpr int kUnrolledPasses = 4;
-
-cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGraphExec_t* out) {
+// One batch as a CUDA graph: the phase kernels of runBatch, every kernel
+// reading its batch from the device cursor, the expand round's leftovers in
+// the cooperative k_expand_rest. One graph launch builds the batch at
+// batchletIndex with no host round trip and no conditional node; a stopped
+// batch (memory, no batch uploaded, time budget) runs through as no-ops.
+cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int restGrid, cudaGraphExec_t* out) {
     *out = nullptr;
-    cudaStream_t cs = nullptr, bs = nullptr;
+    cudaStream_t cs = nullptr;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        if (cs) cudaStreamDestroy(cs);
-        return e;
-    }
+    if (e != cudaSuccess) return e;
     bool capturing = false;
     do {
         if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) break;
         capturing = true;
         k_batch_begin<<<1, 1, 0, cs>>>(d, 1u);
         k_count_first<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
-        cudaStreamCaptureStatus status;
-        cudaGraph_t g = nullptr;
-        const cudaGraphNode_t* deps = nullptr;
-        size_t ndeps = 0;
-        if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &ndeps)) != cudaSuccess) break;
-        cudaGraphConditionalHandle h;
-        if ((e = cudaGraphConditionalHandleCreate(&h, g, 0u, 0u)) != cudaSuccess) break;
-        k_expand_cond<<<1, 1024, 0, cs>>>(d, h, 0u);
-        for (int pass = 0; pass < kUnrolledPasses; pass++) {
-            k_split<<<1, 1024, 0, cs>>>(d, 0u, 1u);
-            k_spill_copy<<<fixedGrid, 256, 0, cs>>>(d, 1u);
-            k_recount<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u, 0u, 1u);
-            k_expand_cond<<<1, 1024, 0, cs>>>(d, h, 1u);
-        }
-        if ((e = cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &ndeps)) != cudaSuccess) break;
-        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t cond;
-        if ((e = cudaGraphAddNode(&cond, g, deps, ndeps, &cp)) != cudaSuccess) break;
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        if ((e = cudaStreamUpdateCaptureDependencies(cs, &cond, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
-            break;
-        // the loop body: split, make room, recount, decide
-        if ((e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
-            cudaSuccess)
-            break;
-        k_split<<<1, 1024, 0, bs>>>(d, 0u, 0u);
-        k_spill_copy<<<fixedGrid, 256, 0, bs>>>(d, 0u);
-        k_recount<<<pointGrid, 256, 0, bs>>>(d, nullptr, 0u, 0u, 0u);
-        k_expand_cond<<<1, 1024, 0, bs>>>(d, h, 0u);
-        cudaGraph_t bodyOut = nullptr;
-        if ((e = cudaStreamEndCapture(bs, &bodyOut)) != cudaSuccess) break;
+        k_deep_book<<<1, 1024, 0, cs>>>(d);
+        k_deep_bin<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        k_deep_split<<<1, 1024, 0, cs>>>(d);
+        k_deep_move<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        if ((e = launchExpandRest(d, restGrid, cs)) != cudaSuccess) break;
         k_zero_grids<<<fixedGrid, 256, 0, cs>>>(d);
         k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         k_vox_commit<<<fixedGrid, 256, 0, cs>>>(d);
@@ -1626,6 +2080,7 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         k_insert<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         k_vox_store<<<fixedGrid, 256, 0, cs>>>(d);
         k_batch_end<<<1, 1, 0, cs>>>(d, kNone);
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
         capturing = false;
         if ((e = cudaStreamEndCapture(cs, &graph)) != cudaSuccess) break;
         e = cudaGraphInstantiate(out, graph, 0ull);
@@ -1636,7 +2091,6 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, cudaGr
         if (dropped) cudaGraphDestroy(dropped);
     }
     if (graph) cudaGraphDestroy(graph);
-    cudaStreamDestroy(bs);
     cudaStreamDestroy(cs);
     if (e != cudaSuccess) {
         cudaGetLastError();

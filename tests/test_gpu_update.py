@@ -96,12 +96,15 @@ def test_host_loop_and_device_graph_agree(c1_cloud, c1_pair):
     for f in ("num_points", "num_voxels", "num_nodes", "expand_iters", "nodes_split", "spilled_points",
               "persistent_offset", "num_allocated_chunks", "chunk_pool_size", "batchlet_index"):
         assert getattr(a, f) == getattr(b, f), f
-    # both paths count the same kernels per batch; the graph adds its loop test
+    # both paths run the same kernels per batch and the same per-iteration
+    # expand passes: on the host as launches, in the graph inside k_expand_rest
     pa = {k: v["launches"] for k, v in host.profile().items()}
     pb = {k: v["launches"] for k, v in ctx.profile().items()}
-    for k in ("k_count_first", "k_split", "k_spill_copy", "k_vox_sample", "k_insert", "k_batch_end"):
+    for k in ("k_count_first", "k_deep_book", "k_deep_bin", "k_deep_split", "k_deep_move", "k_vox_sample",
+              "k_insert", "k_batch_end", "expand_pass"):
         assert pa[k] == pb[k], (k, pa[k], pb[k])
-    assert pb["k_expand_cond"] == pb["k_count_first"] + pb["k_split"]
+    assert pa["k_split"] == pa["k_expand_cond"] == pa["expand_pass"]
+    assert pb["k_expand_rest"] == pb["k_count_first"] == 8 and pb["k_split"] == 0
 
 
 def test_device_time_budget_paces_but_keeps_the_tree(c1_cloud, c1_pair):

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define RB_ABI_VERSION 1u
+#define RB_ABI_VERSION 2u
 
 typedef int32_t rb_status;
 enum {
@@ -133,7 +133,12 @@ typedef struct rb_frame {
     uint32_t enable_edl;
     float edl_strength;              /* 0.4 */
     uint64_t frame_counter;
+    int32_t color_mode;              /* RB_COLOR_* (SharedUniforms::colorMode) */
+    uint32_t show_bounding_box;      /* draw the draw items' boxes after EDL (remo_lines.cuh:120-137) */
 } rb_frame;
+
+/* Sample colour modes (include/remo/HostDeviceCommon.h:63-66). */
+enum { RB_COLOR_RGB = 0, RB_COLOR_BY_NODE = 1, RB_COLOR_BY_LOD = 2, RB_COLOR_WHITE = 3 };
 
 typedef struct rb_build_result {
     uint32_t batches_consumed;       /* Stats::batchletIndex after the call */

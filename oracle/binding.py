@@ -141,6 +141,7 @@ class Frame(ctypes.Structure):
         ("point_size", ctypes.c_int32),
         ("drawlist_capacity", ctypes.c_uint32),
         ("force_large", ctypes.c_void_p),
+        ("color_mode", ctypes.c_int32),
     ]
 
 
@@ -191,6 +192,7 @@ def lib():
         L.or_analysis_scores.argtypes = [vp, ctypes.POINTER(Frame), ctypes.POINTER(AnalysisParams), vp, vp, vp, vp, vp]
         L.or_render_flat.argtypes = [vp, u64, ctypes.POINTER(Frame), vp]
         L.or_edl.argtypes = [vp, u32, u32, ctypes.c_float]
+        L.or_wireframe.argtypes = [vp, ctypes.POINTER(Frame), vp, vp, u32]
         _lib = L
     return _lib
 
@@ -340,6 +342,14 @@ class Tree:
         lib().or_render(self.h, ctypes.byref(frame), _ptr(fb), ctypes.byref(r),
                         _ptr(items) if items is not None else None)
         return fb, r, items
+
+
+def wireframe(tree, frame, fb, item_nodes):
+    """The draw items' box edges drawn into fb (a copy is returned)."""
+    out = np.array(fb, dtype=np.uint64, copy=True)
+    items = np.ascontiguousarray(item_nodes, dtype=np.uint32)
+    lib().or_wireframe(tree.h, ctypes.byref(frame), _ptr(out), _ptr(items), len(items))
+    return out
 
 
 def render_flat(points, frame):

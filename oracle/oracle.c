@@ -1161,6 +1161,28 @@ static void draw_point(uint64_t* fb, const or_frame* f, float x, float y, float 
     }
 }
 
+/* remoHashColor (kernels/shared/remo_prelude.cuh:87-97) */
+static uint32_t hash_color(uint64_t key) {
+    uint64_t h = (key + 0x9E3779B97F4A7C15ull) * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 32;
+    uint32_t r = 96u + (((uint32_t)h & 0xFFu) * 159u) / 255u;
+    uint32_t g = 96u + (((uint32_t)(h >> 8) & 0xFFu) * 159u) / 255u;
+    uint32_t b = 96u + (((uint32_t)(h >> 16) & 0xFFu) * 159u) / 255u;
+    return r | (g << 8) | (b << 16) | (255u << 24);
+}
+
+/* remoSampleColor (remo_draw.cuh:104-116); the item key is the node's index */
+static uint32_t sample_color(int32_t mode, uint32_t node, uint32_t level, uint32_t rgba) {
+    switch (mode) {
+        case 1: return hash_color(node);
+        case 2: return hash_color((uint64_t)level * 2654435761ull);
+        case 3: return 0xFFFFFFFFu;
+        default: return rgba;
+    }
+}
+
 void or_render(const or_tree* t, const or_frame* f, uint64_t* fb, or_render_result* r,
                uint32_t* item_nodes) {
     const uint64_t npx = (uint64_t)f->width * (uint64_t)f->height;
@@ -1219,17 +1241,101 @@ void or_render(const or_tree* t, const or_frame* f, uint64_t* fb, or_render_resu
             /* the walker stops at the end of the chunk list (remo_draw.cuh:78-102) */
             uint32_t np = tn->num_points, pc = tn->num_point_chunks * ppc;
             if (np > pc) np = pc;
+            const uint32_t tid = targets[k];
             for (uint32_t s = 0; s < np; s++)
-                draw_point(fb, f, tn->pts[s].x, tn->pts[s].y, tn->pts[s].z, tn->pts[s].color);
+                draw_point(fb, f, tn->pts[s].x, tn->pts[s].y, tn->pts[s].z,
+                           sample_color(f->color_mode, tid, tn->level, tn->pts[s].color));
             uint32_t nv = tn->num_voxels, vc = tn->num_voxel_chunks * ppc;
             if (nv > vc) nv = vc;
             if (nv > tn->num_voxels_stored) nv = tn->num_voxels_stored;
             for (uint32_t s = 0; s < nv; s++)
-                draw_point(fb, f, tn->vox[s].x, tn->vox[s].y, tn->vox[s].z, tn->vox[s].color);
+                draw_point(fb, f, tn->vox[s].x, tn->vox[s].y, tn->vox[s].z,
+                           sample_color(f->color_mode, tid, tn->level, tn->vox[s].color));
         }
     }
     free(vis);
     free(large);
+}
+
+/* remoClipSegment2D (remo_lines.cuh:30-55), one boundary */
+static int clip_test(float p, float q, float* t0, float* t1) {
+    if (p == 0.0f) return q >= 0.0f;
+    float r = q / p;
+    if (p < 0.0f) {
+        if (r > *t1) return 0;
+        if (r > *t0) *t0 = r;
+    } else {
+        if (r < *t0) return 0;
+        if (r < *t1) *t1 = r;
+    }
+    return 1;
+}
+
+/* remoDrawSegment (remo_lines.cuh:57-117) */
+static void draw_segment(uint64_t* fb, const or_frame* f, const float a[3], const float b[3], uint32_t color) {
+    f4 c0 = matmul(f->transform, a[0], a[1], a[2], 1.0f);
+    f4 c1 = matmul(f->transform, b[0], b[1], b[2], 1.0f);
+    const float min_w = 1.0e-6f;
+    if (c0.w < min_w && c1.w < min_w) return;
+    if (c0.w < min_w) {
+        float t = (min_w - c0.w) / (c1.w - c0.w);
+        f4 c = {c0.x + t * (c1.x - c0.x), c0.y + t * (c1.y - c0.y), c0.z + t * (c1.z - c0.z), min_w};
+        c0 = c;
+    } else if (c1.w < min_w) {
+        float t = (min_w - c1.w) / (c0.w - c1.w);
+        f4 c = {c1.x + t * (c0.x - c1.x), c1.y + t * (c0.y - c1.y), c1.z + t * (c0.z - c1.z), min_w};
+        c1 = c;
+    }
+    float iw0 = 1.0f / c0.w, iw1 = 1.0f / c1.w;
+    float sx0 = (c0.x * iw0 * 0.5f + 0.5f) * f->width, sy0 = (c0.y * iw0 * 0.5f + 0.5f) * f->height;
+    float sx1 = (c1.x * iw1 * 0.5f + 0.5f) * f->width, sy1 = (c1.y * iw1 * 0.5f + 0.5f) * f->height;
+    int32_t W = cvt_s32(f->width), H = cvt_s32(f->height);
+    if (W <= 0 || H <= 0) return;
+    float dx = sx1 - sx0, dy = sy1 - sy0, t0 = 0.0f, t1 = 1.0f;
+    if (!clip_test(-dx, sx0, &t0, &t1) || !clip_test(dx, (float)(W - 1) - sx0, &t0, &t1) ||
+        !clip_test(-dy, sy0, &t0, &t1) || !clip_test(dy, (float)(H - 1) - sy0, &t0, &t1))
+        return;
+    float ax = sx0 + t0 * (sx1 - sx0), ay = sy0 + t0 * (sy1 - sy0);
+    float bx = sx0 + t1 * (sx1 - sx0), by = sy0 + t1 * (sy1 - sy0);
+    int32_t steps = cvt_s32(fmaxf(fabsf(bx - ax), fabsf(by - ay))) + 1;
+    float inv_steps = 1.0f / (float)steps;
+    for (int32_t st = 0; st <= steps; st++) {
+        float q = (float)st * inv_steps;
+        int32_t ix = cvt_s32(ax + q * (bx - ax)), iy = cvt_s32(ay + q * (by - ay));
+        if (ix < 0 || iy < 0 || ix >= W || iy >= H) continue;
+        float s_t = t0 + q * (t1 - t0);
+        float iw = iw0 + s_t * (iw1 - iw0);
+        if (!(iw > 0.0f)) continue;
+        float depth = 1.0f / iw;
+        uint32_t bits;
+        memcpy(&bits, &depth, 4);
+        uint64_t packed = ((uint64_t)bits << 32) | color;
+        uint64_t* px = &fb[(uint64_t)iy * (uint64_t)W + (uint64_t)ix];
+        if (packed < *px) *px = packed;
+    }
+}
+
+void or_wireframe(const or_tree* t, const or_frame* f, uint64_t* fb, const uint32_t* item_nodes, uint32_t n) {
+    float cube = fmaxf(fmaxf(f->box_max[0] - f->box_min[0], f->box_max[1] - f->box_min[1]),
+                       f->box_max[2] - f->box_min[2]);
+    for (uint32_t k = 0; k < n; k++) {
+        const onode* nd = &t->nodes[item_nodes[k]];
+        float mn[3], mx[3], size;
+        node_bounds(f, nd, cube, mn, mx, &size);
+        if (!(size > 0.0f)) continue;
+        uint32_t color = hash_color((uint64_t)nd->level * 2654435761ull);
+        /* remoBoxEdge (remo_lines.cuh:11-27) */
+        for (uint32_t e = 0; e < 12; e++) {
+            uint32_t axis = e / 4u, rest = e % 4u;
+            float off[3] = {0.0f, 0.0f, 0.0f};
+            off[(axis + 1u) % 3u] = (rest & 1u) ? size : 0.0f;
+            off[(axis + 2u) % 3u] = (rest & 2u) ? size : 0.0f;
+            float a[3] = {mn[0] + off[0], mn[1] + off[1], mn[2] + off[2]};
+            off[axis] = size;
+            float b[3] = {mn[0] + off[0], mn[1] + off[1], mn[2] + off[2]};
+            draw_segment(fb, f, a, b, color);
+        }
+    }
 }
 
 void or_render_flat(const or_point* pts, uint64_t n, const or_frame* f, uint64_t* fb) {

@@ -202,6 +202,9 @@ struct or_frame {
     uint32_t drawlist_capacity;  /* 131072 (remolod_render.cu:22) */
     /* optional: nodes forced large (Refinement); NULL or num_nodes bytes */
     const uint8_t* force_large;
+    /* SharedUniforms::colorMode (HostDeviceCommon.h:63-66): 0 rgb, 1 by node,
+     * 2 by level, 3 white */
+    int32_t color_mode;
 };
 
 typedef struct or_render_result {
@@ -220,6 +223,9 @@ void or_render(const or_tree* t, const or_frame* f, uint64_t* fb, or_render_resu
 void or_render_flat(const or_point* pts, uint64_t n, const or_frame* f, uint64_t* fb);
 /* remo_framebuffer.cuh:78-122 with libm log2f/expf in place of the intrinsics. */
 void or_edl(uint64_t* fb, uint32_t width, uint32_t height, float strength);
+/* remoDrawListWireframe (remo_lines.cuh:120-137): the 12 box edges of each of
+ * the n draw items' nodes, drawn into fb (after EDL in the reference). */
+void or_wireframe(const or_tree* t, const or_frame* f, uint64_t* fb, const uint32_t* item_nodes, uint32_t n);
 
 #ifdef __cplusplus
 }

@@ -18,6 +18,7 @@ RB_ERR_RING, RB_ERR_CAPACITY, RB_ERR_NO_DEVICE, RB_ERR_UNSUPPORTED = 5, 6, 7, 8
 RB_PIPELINE_REMOLOD, RB_PIPELINE_SIMLOD, RB_PIPELINE_FLAT = 0, 1, 2
 RB_VOXEL_LOWEST_INDEX, RB_VOXEL_FIRST_COME = 0, 1
 RB_SCORE_PARTIAL, RB_SCORE_CLOSED, RB_SCORE_LEARNED = 0, 1, 2
+RB_COLOR_RGB, RB_COLOR_BY_NODE, RB_COLOR_BY_LOD, RB_COLOR_WHITE = 0, 1, 2, 3
 MLP_NUM_PARAMS, NUM_FEATURES = 5378, 16
 
 u32, u64, i32, f32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_float
@@ -45,7 +46,8 @@ class BatchView(ctypes.Structure):
 class Frame(ctypes.Structure):
     _fields_ = [("width", f32), ("height", f32), ("transform", f32 * 16), ("transform_frozen", f32 * 16),
                 ("box_min", f32 * 3), ("box_max", f32 * 3), ("lod_pixel_budget", f32), ("point_size", i32),
-                ("enable_edl", u32), ("edl_strength", f32), ("frame_counter", u64)]
+                ("enable_edl", u32), ("edl_strength", f32), ("frame_counter", u64), ("color_mode", i32),
+                ("show_bounding_box", u32)]
 
 
 class BuildResult(ctypes.Structure):

@@ -29,7 +29,7 @@ enum KernelId : int {
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
     K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_PASS, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE,
-    K_EXPAND_REST, K_NUM
+    K_EXPAND_REST, K_WIREFRAME, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
@@ -39,7 +39,8 @@ static const char* const kKernelNames[K_NUM] = {
     "k_queue", "k_refine", "k_score", "k_mlp_predict", "k_mlp_grad", "k_mlp_adam",
     "k_expand_cond", "k_zero_grids",
     // not a kernel: per-iteration expand passes run inside k_expand_rest
-    "expand_pass", "k_deep_book", "k_deep_bin", "k_deep_split", "k_deep_move", "k_expand_rest"};
+    "expand_pass", "k_deep_book", "k_deep_bin", "k_deep_split", "k_deep_move", "k_expand_rest",
+    "k_wireframe"};
 
 struct Profiler {
     bool on = false;
@@ -881,6 +882,8 @@ static rb::Frame toFrame(const rb_frame* f) {
     }
     r.lodPixelBudget = f->lod_pixel_budget;
     r.pointSize = f->point_size;
+    r.colorMode = f->color_mode;
+    r.showBoundingBox = f->show_bounding_box;
     return r;
 }
 
@@ -920,7 +923,14 @@ rb_status rb_render(rb_ctx* c, const rb_frame* f, uint64_t fbDev, uint64_t rgbaD
     LAUNCH(c, K_FRONTIER, 0, rb::launchFrontier(c->d, c->vis, c->large, c->rs, c->items, cap, c->numSMs * 4,
                                                 c->stream));
     LAUNCH(c, K_RASTER, 0, rb::launchRaster(c->d, fr, fb, c->rs, c->items, cap, c->numSMs * 8, c->stream));
-    rb_status st = finishFrame(c, f, fb, reinterpret_cast<uint32_t*>(rgbaDev), npx);
+    // EDL, then the boxes (remolod_render.cu:183-189), then the resolve
+    rb_status st = finishFrame(c, f, fb, nullptr, npx);
+    if (st != RB_OK) return st;
+    if (f->show_bounding_box)
+        LAUNCH(c, K_WIREFRAME, 0, rb::launchWireframe(c->d, fr, fb, c->rs, c->items, cap, c->numSMs * 8, c->stream));
+    if (rgbaDev)
+        LAUNCH(c, K_RESOLVE, npx, rb::launchResolve(fb, reinterpret_cast<uint32_t*>(rgbaDev), npx, c->numSMs * 8,
+                                                    c->stream));
     if (st != RB_OK) return st;
     RB_CUDA(c, cudaGetLastError());
     RB_CUDA(c, cudaEventRecord(c->evStop, c->stream));

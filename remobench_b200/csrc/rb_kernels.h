@@ -18,6 +18,8 @@ struct Frame {
     float boxMin[3], boxMax[3];
     float lodPixelBudget;
     int32_t pointSize;
+    int32_t colorMode;          // 0 rgb, 1 by node, 2 by level, 3 white
+    uint32_t showBoundingBox;
 };
 
 struct RenderScratch {
@@ -71,5 +73,8 @@ void launchRasterFlat(const Frame& f, unsigned long long* fb, const Point* pts, 
 void launchEdl(const unsigned long long* src, unsigned long long* dst, uint32_t w, uint32_t h,
                float strength, int grid, cudaStream_t s);
 void launchResolve(const unsigned long long* fb, uint32_t* rgba, uint64_t npx, int grid, cudaStream_t s);
+// The draw items' bounding boxes as lines (remo_lines.cuh:120-137), after EDL.
+void launchWireframe(const Dev& d, const Frame& f, unsigned long long* fb, const RenderScratch* rs,
+                     const uint32_t* items, uint32_t cap, int grid, cudaStream_t s);
 
 }  // namespace rb

@@ -121,6 +121,8 @@ rb_status renderNoalloc(rb_ctx* ctx, const rb::CtxRenderAccess& a, unsigned char
     }
     fr.lodPixelBudget = f->lod_pixel_budget;
     fr.pointSize = f->point_size;
+    fr.colorMode = f->color_mode;
+    fr.showBoundingBox = f->show_bounding_box;
 
     cudaError_t e;
     cudaStream_t s = a.stream;
@@ -132,6 +134,7 @@ rb_status renderNoalloc(rb_ctx* ctx, const rb::CtxRenderAccess& a, unsigned char
     rb::launchRaster(a.d, fr, fb, rs, items, cap, a.numSMs * 8, s);
     if (f->enable_edl) rb::launchEdl(fb, fb, (uint32_t)f->width, (uint32_t)f->height, f->edl_strength,
                                      a.numSMs * 8, s);
+    if (f->show_bounding_box) rb::launchWireframe(a.d, fr, fb, rs, items, cap, a.numSMs * 8, s);
     if (rgbaDev) rb::launchResolve(fb, reinterpret_cast<uint32_t*>(rgbaDev), npx, a.numSMs * 8, s);
     if ((e = cudaGetLastError()) != cudaSuccess) return cudaFail(ctx, "kernel launch", e);
     if ((e = cudaEventRecord(a.evStop, s)) != cudaSuccess) return cudaFail(ctx, "cudaEventRecord", e);

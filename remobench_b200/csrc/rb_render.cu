@@ -207,6 +207,27 @@ __global__ void __launch_bounds__(256) k_frontier(Dev d, const uint8_t* vis, con
     }
 }
 
+// remoHashColor (kernels/shared/remo_prelude.cuh:87-97): a splitmix-style
+// hash of the key, each channel mapped to [96, 255], alpha 255.
+__device__ __forceinline__ uint32_t hashColor(unsigned long long key) {
+    unsigned long long h = (key + 0x9E3779B97F4A7C15ull) * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 32;
+    const uint32_t r = 96u + (((uint32_t)h & 0xFFu) * 159u) / 255u;
+    const uint32_t g = 96u + (((uint32_t)(h >> 8) & 0xFFu) * 159u) / 255u;
+    const uint32_t b = 96u + (((uint32_t)(h >> 16) & 0xFFu) * 159u) / 255u;
+    return r | (g << 8) | (b << 16) | (255u << 24);
+}
+
+// remoSampleColor (remo_draw.cuh:104-116): the colour every sample of a draw
+// item takes in the non-RGB modes; the item key is the node's pool index.
+__device__ __forceinline__ uint32_t itemColor(int32_t mode, uint32_t node, uint32_t level) {
+    if (mode == 3) return 0xFFFFFFFFu;
+    if (mode == 1) return hashColor(node);
+    return hashColor((unsigned long long)level * 2654435761ull);
+}
+
 // remoRasterizeDrawList (remo_draw.cuh:118-167): one block per draw item; the
 // block walks the node's chunks in order, so the loads of a chunk coalesce.
 __global__ void __launch_bounds__(256) k_raster(Dev d, Frame f, unsigned long long* fb,
@@ -217,6 +238,8 @@ __global__ void __launch_bounds__(256) k_raster(Dev d, Frame f, unsigned long lo
     const uint32_t ppc = d.ppc;
     for (uint32_t w = blockIdx.x; w < ni; w += gridDim.x) {
         const uint32_t node = items[w];
+        const bool rgb = f.colorMode < 1 || f.colorMode > 3;
+        const uint32_t fixed = rgb ? 0u : itemColor(f.colorMode, node, d.level[node]);
         uint32_t np = d.numPoints[node];
         const uint32_t pcap = d.numPointChunks[node] * ppc;
         if (np > pcap) np = pcap;
@@ -225,7 +248,7 @@ __global__ void __launch_bounds__(256) k_raster(Dev d, Frame f, unsigned long lo
             const uint32_t phys = d.tablePool[poff + s / ppc];
             if (phys == kNone) continue;
             const float4 v = __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc));
-            drawPoint(fb, f, v.x, v.y, v.z, __float_as_uint(v.w));
+            drawPoint(fb, f, v.x, v.y, v.z, rgb ? __float_as_uint(v.w) : fixed);
         }
         uint32_t nv = d.numVoxels[node];
         const uint32_t vcap = d.numVoxelChunks[node] * ppc;
@@ -236,8 +259,97 @@ __global__ void __launch_bounds__(256) k_raster(Dev d, Frame f, unsigned long lo
             const uint32_t phys = d.tablePool[voff + s / ppc];
             if (phys == kNone) continue;
             const float4 v = __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc));
-            drawPoint(fb, f, v.x, v.y, v.z, __float_as_uint(v.w));
+            drawPoint(fb, f, v.x, v.y, v.z, rgb ? __float_as_uint(v.w) : fixed);
         }
+    }
+}
+
+// remoClipSegment2D (remo_lines.cuh:30-55): Liang-Barsky against
+// [0, xmax] x [0, ymax]; false when the segment misses.
+__device__ __forceinline__ bool clipTest(float p, float q, float& t0, float& t1) {
+    if (p == 0.0f) return q >= 0.0f;
+    const float r = q / p;
+    if (p < 0.0f) {
+        if (r > t1) return false;
+        if (r > t0) t0 = r;
+    } else {
+        if (r < t0) return false;
+        if (r < t1) t1 = r;
+    }
+    return true;
+}
+
+// remoDrawSegment (remo_lines.cuh:57-117): near-plane clip in clip space at
+// w = 1e-6, screen clip, then one sample per step along the longer axis with
+// depth from the interpolated 1/w.
+__device__ void drawSegment(unsigned long long* fb, const Frame& f, float ax0, float ay0, float az0, float bx0,
+                            float by0, float bz0, uint32_t color) {
+    F4 c0 = matmul(f.transform, ax0, ay0, az0, 1.0f);
+    F4 c1 = matmul(f.transform, bx0, by0, bz0, 1.0f);
+    const float kMinW = 1.0e-6f;
+    if (c0.w < kMinW && c1.w < kMinW) return;
+    if (c0.w < kMinW) {
+        const float t = (kMinW - c0.w) / (c1.w - c0.w);
+        c0 = F4{c0.x + t * (c1.x - c0.x), c0.y + t * (c1.y - c0.y), c0.z + t * (c1.z - c0.z), kMinW};
+    } else if (c1.w < kMinW) {
+        const float t = (kMinW - c1.w) / (c0.w - c1.w);
+        c1 = F4{c1.x + t * (c0.x - c1.x), c1.y + t * (c0.y - c1.y), c1.z + t * (c0.z - c1.z), kMinW};
+    }
+    const float invW0 = 1.0f / c0.w, invW1 = 1.0f / c1.w;
+    const float sx0 = (c0.x * invW0 * 0.5f + 0.5f) * f.width;
+    const float sy0 = (c0.y * invW0 * 0.5f + 0.5f) * f.height;
+    const float sx1 = (c1.x * invW1 * 0.5f + 0.5f) * f.width;
+    const float sy1 = (c1.y * invW1 * 0.5f + 0.5f) * f.height;
+    const int32_t W = __float2int_rz(f.width), H = __float2int_rz(f.height);
+    if (W <= 0 || H <= 0) return;
+    const float dx = sx1 - sx0, dy = sy1 - sy0;
+    float t0 = 0.0f, t1 = 1.0f;
+    if (!clipTest(-dx, sx0, t0, t1) || !clipTest(dx, (float)(W - 1) - sx0, t0, t1) || !clipTest(-dy, sy0, t0, t1) ||
+        !clipTest(dy, (float)(H - 1) - sy0, t0, t1))
+        return;
+    const float ax = sx0 + t0 * (sx1 - sx0), ay = sy0 + t0 * (sy1 - sy0);
+    const float bx = sx0 + t1 * (sx1 - sx0), by = sy0 + t1 * (sy1 - sy0);
+    const int32_t steps = __float2int_rz(fmaxf(fabsf(bx - ax), fabsf(by - ay))) + 1;
+    const float invSteps = 1.0f / (float)steps;
+    for (int32_t st = 0; st <= steps; ++st) {
+        const float q = (float)st * invSteps;
+        const int32_t ix = __float2int_rz(ax + q * (bx - ax));
+        const int32_t iy = __float2int_rz(ay + q * (by - ay));
+        if (ix < 0 || iy < 0 || ix >= W || iy >= H) continue;
+        const float sT = t0 + q * (t1 - t0);
+        const float invW = invW0 + sT * (invW1 - invW0);
+        if (!(invW > 0.0f)) continue;
+        const float depth = 1.0f / invW;
+        atomicMin(&fb[(unsigned long long)iy * (unsigned long long)W + (unsigned long long)ix],
+                  ((unsigned long long)__float_as_uint(depth) << 32) | (unsigned long long)color);
+    }
+}
+
+// remoDrawListWireframe (remo_lines.cuh:120-137): the 12 edges of every draw
+// item's node box (remoBoxEdge, :11-27: edge / 4 is the axis the edge runs
+// along, edge % 4 picks the offsets on the other two), coloured by level.
+__global__ void __launch_bounds__(256) k_wireframe(Dev d, Frame f, unsigned long long* fb,
+                                                   const RenderScratch* rs, const uint32_t* items, uint32_t cap) {
+    uint32_t ni = rs->numItems;
+    if (ni > cap) ni = cap;
+    const float cube = fmaxf(fmaxf(f.boxMax[0] - f.boxMin[0], f.boxMax[1] - f.boxMin[1]), f.boxMax[2] - f.boxMin[2]);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < (uint64_t)ni * 12u;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t node = items[i / 12u];
+        const uint32_t edge = (uint32_t)(i % 12u);
+        const uint32_t lv = d.level[node];
+        const float size = cube / __int_as_float((int)((127u + lv) << 23));
+        if (!(size > 0.0f)) continue;
+        const float mn[3] = {f.boxMin[0] + (float)d.nodeX[node] * size, f.boxMin[1] + (float)d.nodeY[node] * size,
+                             f.boxMin[2] + (float)d.nodeZ[node] * size};
+        const uint32_t axis = edge / 4u, rest = edge % 4u;
+        float off[3] = {0.0f, 0.0f, 0.0f};
+        off[(axis + 1u) % 3u] = (rest & 1u) ? size : 0.0f;
+        off[(axis + 2u) % 3u] = (rest & 2u) ? size : 0.0f;
+        const float a[3] = {mn[0] + off[0], mn[1] + off[1], mn[2] + off[2]};
+        off[axis] = size;
+        drawSegment(fb, f, a[0], a[1], a[2], mn[0] + off[0], mn[1] + off[1], mn[2] + off[2],
+                    hashColor((unsigned long long)lv * 2654435761ull));
     }
 }
 
@@ -323,6 +435,10 @@ void launchEdl(const unsigned long long* src, unsigned long long* dst, uint32_t 
 }
 void launchResolve(const unsigned long long* fb, uint32_t* rgba, uint64_t npx, int grid, cudaStream_t s) {
     k_resolve<<<grid, 256, 0, s>>>(fb, rgba, npx);
+}
+void launchWireframe(const Dev& d, const Frame& f, unsigned long long* fb, const RenderScratch* rs,
+                     const uint32_t* items, uint32_t cap, int grid, cudaStream_t s) {
+    k_wireframe<<<grid, 256, 0, s>>>(d, f, fb, rs, items, cap);
 }
 
 }  // namespace rb

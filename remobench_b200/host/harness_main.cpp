@@ -50,6 +50,8 @@ struct Options {
     std::string surfaceOut;
     bool strictTiming = false;
     bool trace = false;
+    bool boxes = false;     // the viewer's bounding-box toggle (SharedUniforms::showBoundingBox)
+    int colorMode = 0;      // SharedUniforms::colorMode: rgb, node, lod, white
 };
 
 void usage() {
@@ -57,7 +59,8 @@ void usage() {
                  "usage: rb_harness [--pipeline ID] [--synthetic N] [--config C] [--seed S] [--batch B]\n"
                  "                  [--size W H] [--device-budget GB] [--device D] [--dump-frame PATH]\n"
                  "                  [--dump-after F] [--switch-to ID] [--switch-after F] [--max-frames F]\n"
-                 "                  [--frame-file PATH] [--surface-out PATH] [--strict-timing] [--trace]\n");
+                 "                  [--frame-file PATH] [--surface-out PATH] [--strict-timing] [--trace]\n"
+                 "                  [--bounding-boxes] [--color-mode rgb|node|lod|white]\n");
 }
 
 bool parse(int argc, char** argv, Options* o) {
@@ -125,6 +128,19 @@ bool parse(int argc, char** argv, Options* o) {
             o->strictTiming = true;
         } else if (a == "--trace") {
             o->trace = true;
+        } else if (a == "--bounding-boxes") {
+            o->boxes = true;
+        } else if (a == "--color-mode") {
+            if (!(v = next("--color-mode"))) return false;
+            const std::string m = v;
+            const char* modes[] = {"rgb", "node", "lod", "white"};
+            o->colorMode = -1;
+            for (int k = 0; k < 4; k++)
+                if (m == modes[k]) o->colorMode = k;
+            if (o->colorMode < 0) {
+                std::fprintf(stderr, "rb_harness: --color-mode takes rgb, node, lod or white\n");
+                return false;
+            }
         } else {
             std::fprintf(stderr, "rb_harness: unknown option %s\n", a.c_str());
             usage();
@@ -399,6 +415,8 @@ int main(int argc, char** argv) {
         fc.uniforms = haveFixed ? fixedUniforms
                                 : orbitFrame(meta, opt.width, opt.height, 0.35 + 0.02 * frame, -0.6, uint64_t(frame));
         fc.uniforms.frame_counter = uint64_t(frame);
+        if (opt.boxes) fc.uniforms.show_bounding_box = 1;
+        if (opt.colorMode) fc.uniforms.color_mode = opt.colorMode;
         fc.targets.surface = reinterpret_cast<uint64_t>(surface);
         fc.targets.width = opt.width;
         fc.targets.height = opt.height;

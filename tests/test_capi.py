@@ -31,7 +31,7 @@ def test_every_declared_symbol_is_exported():
 
 def test_abi_version_and_status_strings():
     lib = capi.lib()
-    assert lib.rb_abi_version() == 1
+    assert lib.rb_abi_version() == 2
     assert lib.rb_status_string(0) == b"ok"
     assert lib.rb_status_string(5) == b"ring depth mismatch"
 

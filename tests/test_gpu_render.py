@@ -87,3 +87,31 @@ def test_edl_within_one_step(c1_trees):
     gc = (g & 0xFFFFFFFF).astype(np.uint32).view(np.uint8).reshape(-1, 4).astype(np.int32)
     oc = (oe & 0xFFFFFFFF).astype(np.uint32).view(np.uint8).reshape(-1, 4).astype(np.int32)
     assert np.max(np.abs(gc - oc)) <= 1  # libm vs CUDA log2f/expf: at most one 8-bit step
+
+
+@pytest.mark.parametrize("mode", [1, 2, 3])
+def test_colour_modes_and_bounding_boxes_bit_exact(c1_trees, mode):
+    """The reference viewer's colour modes (by node, by level, white;
+    remo_draw.cuh:104-116) and its bounding-box wireframe drawn over the frame
+    (remo_lines.cuh:120-137): the framebuffer with the boxes equals the
+    oracle's render followed by its wireframe over the same draw items."""
+    import torch
+    from remobench_b200.lod import make_frame
+    ctx, tree, bmin, bmax = c1_trees
+    f = make_frame(bmin, bmax, W, H, yaw=0.8, pitch=-0.5, radius_scale=0.45)
+    f.color_mode = mode
+    f.show_bounding_box = 1
+    fb = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    r = ctx.render(f, fb)
+    of = oracle_frame(f)
+    of.color_mode = mode
+    ofb, orr, items = tree.render(of, item_nodes_cap=131072)
+    assert r.draw_items == orr.draw_items > 0
+    ofb = ob.wireframe(tree, of, ofb, items[:orr.draw_items])
+    g = fb.cpu().numpy().view(np.uint64)
+    assert np.array_equal(g, ofb)
+    # the boxes drew something the points did not: line colours of the levels present
+    f.show_bounding_box = 0
+    fb2 = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    ctx.render(f, fb2)
+    assert np.count_nonzero(fb2.cpu().numpy().view(np.uint64) != g) > 1000

@@ -9,7 +9,7 @@
 //              [--batch B] [--size W H] [--device-budget GB] [--device D]
 //              [--dump-frame out.ppm] [--dump-after F] [--switch-to ID] [--switch-after F]
 //              [--max-frames F] [--frame-file uniforms.bin] [--surface-out rgba.bin]
-//              [--strict-timing] [--trace]
+//              [--strict-timing] [--trace] [--bounding-boxes] [--color-mode M] [--file cloud.simlod]
 //
 // Without --dump-after the loop runs until the build is complete (or stops on
 // memCapacityReached), renders one more frame and stops. The last stdout line
@@ -50,6 +50,7 @@ struct Options {
     std::string surfaceOut;
     bool strictTiming = false;
     bool trace = false;
+    std::string file;       // a .simlod cloud streamed from disk instead of the generator
     bool boxes = false;     // the viewer's bounding-box toggle (SharedUniforms::showBoundingBox)
     int colorMode = 0;      // SharedUniforms::colorMode: rgb, node, lod, white
 };
@@ -60,7 +61,7 @@ void usage() {
                  "                  [--size W H] [--device-budget GB] [--device D] [--dump-frame PATH]\n"
                  "                  [--dump-after F] [--switch-to ID] [--switch-after F] [--max-frames F]\n"
                  "                  [--frame-file PATH] [--surface-out PATH] [--strict-timing] [--trace]\n"
-                 "                  [--bounding-boxes] [--color-mode rgb|node|lod|white]\n");
+                 "                  [--bounding-boxes] [--color-mode rgb|node|lod|white] [--file PATH.simlod]\n");
 }
 
 bool parse(int argc, char** argv, Options* o) {
@@ -128,6 +129,9 @@ bool parse(int argc, char** argv, Options* o) {
             o->strictTiming = true;
         } else if (a == "--trace") {
             o->trace = true;
+        } else if (a == "--file") {
+            if (!(v = next("--file"))) return false;
+            o->file = v;
         } else if (a == "--bounding-boxes") {
             o->boxes = true;
         } else if (a == "--color-mode") {
@@ -344,7 +348,8 @@ int main(int argc, char** argv) {
     std::string err;
     const auto tGen = std::chrono::steady_clock::now();
     std::unique_ptr<PointSource> source =
-        makeSyntheticSource(opt.config, opt.synthetic, opt.seed, opt.batch, opt.device, &err);
+        opt.file.empty() ? makeSyntheticSource(opt.config, opt.synthetic, opt.seed, opt.batch, opt.device, &err)
+                         : makeSimlodSource(opt.file, opt.batch, opt.device, &err);
     if (!source) {
         std::fprintf(stderr, "rb_harness: %s\n", err.c_str());
         return 1;

@@ -11,7 +11,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 
+#include "simlod_file.h"
 #include "synth.h"
 
 namespace rbhost {
@@ -34,6 +36,13 @@ static uint32_t batchCount(uint64_t numPoints, uint32_t batch) {
     return static_cast<uint32_t>((numPoints + batch - 1) / batch);
 }
 
+// Reads points [first, first + count) of the cloud into dst (host memory).
+using RangeReader = std::function<bool(uint64_t first, uint64_t count, rb_point* dst, std::string* err)>;
+
+// A cloud fed to the device ring either from host memory (uploaded straight
+// from its registered pages) or from a reader that fills a pinned staging
+// batch per upload (a .simlod file streamed from disk, as the reference's
+// SimlodFileProducer does).
 class MemorySource final : public PointSource {
 public:
     MemorySource(std::vector<rb_point> points, const CloudMeta& meta, uint32_t batchSize, int device)
@@ -41,9 +50,13 @@ public:
           m_device(device) {
         m_meta.numPoints = m_points.size();
     }
+    MemorySource(RangeReader reader, const CloudMeta& meta, uint32_t batchSize, int device)
+        : m_reader(std::move(reader)), m_meta(meta),
+          m_batch(std::max<uint32_t>(1, std::min(batchSize, kSlotCapacity))), m_device(device) {}
     ~MemorySource() override {
         stop();
         if (m_registered) cudaHostUnregister(m_points.data());
+        if (m_staging) cudaFreeHost(m_staging);
         if (m_stream) cudaStreamDestroy(m_stream);
     }
 
@@ -85,12 +98,20 @@ public:
             if (err) *err = "cudaStreamCreate failed";
             return false;
         }
-        if (!m_registered) {
+        if (!m_reader && !m_registered) {
             // Pinned pages make the uploads run at full PCIe / C2C rate; pageable
             // copies still work if registration is refused.
             m_registered = cudaHostRegister(m_points.data(), m_points.size() * sizeof(rb_point),
                                             cudaHostRegisterDefault) == cudaSuccess;
             if (!m_registered) cudaGetLastError();
+        }
+        if (m_reader && !m_staging &&
+            cudaMallocHost(reinterpret_cast<void**>(&m_staging), uint64_t(kSlotCapacity) * sizeof(rb_point)) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            m_staging = nullptr;
+            if (err) *err = "cudaMallocHost failed for the file staging batch";
+            return false;
         }
         void* p = nullptr;
         if (cudaMalloc(&p, bytes) != cudaSuccess) {
@@ -183,8 +204,18 @@ private:
         const uint32_t slot = static_cast<uint32_t>(b % m_numSlots);
         const uint64_t stride = m_mode == Mode::Whole ? m_curBatch : kSlotCapacity;
         rb_point* dst = reinterpret_cast<rb_point*>(m_slots) + uint64_t(slot) * stride;
-        if (cudaMemcpyAsync(dst, m_points.data() + first, count * sizeof(rb_point), cudaMemcpyHostToDevice,
-                            m_stream) != cudaSuccess)
+        const rb_point* src = m_points.data() + first;
+        if (m_reader) {
+            // the staging batch is reused: the previous upload must be done
+            if (cudaStreamSynchronize(m_stream) != cudaSuccess) return false;
+            std::string err;
+            if (!m_reader(first, count, m_staging, &err)) {
+                std::fprintf(stderr, "rbhost: %s\n", err.c_str());
+                return false;
+            }
+            src = m_staging;
+        }
+        if (cudaMemcpyAsync(dst, src, count * sizeof(rb_point), cudaMemcpyHostToDevice, m_stream) != cudaSuccess)
             return false;
         m_sizes[slot] = static_cast<uint32_t>(count);
         m_uploaded += count;
@@ -192,6 +223,8 @@ private:
     }
 
     std::vector<rb_point> m_points;
+    RangeReader m_reader;
+    rb_point* m_staging = nullptr;  // pinned, one slot of points (reader sources)
     CloudMeta m_meta;
     uint32_t m_batch;
     int m_device;
@@ -251,6 +284,29 @@ std::unique_ptr<PointSource> makeSyntheticSource(int config, uint64_t numPoints,
         return nullptr;
     }
     return makeMemorySource(std::move(pts), meta, cfg.batch_size, device);
+}
+
+std::unique_ptr<PointSource> makeSimlodSource(const std::string& path, uint32_t batchSize, int device,
+                                              std::string* err) {
+    SimlodInfo info;
+    if (!readSimlodHeader(path, info, err)) return nullptr;
+    // the observed box, not the header's (src/io/PointSource.cpp:515-531)
+    double bounds[6];
+    if (!readSimlodBounds(path, info, bounds, err)) return nullptr;
+    CloudMeta meta;
+    meta.numPoints = info.numPoints;
+    for (int a = 0; a < 3; a++) {
+        meta.boxMinOrig[a] = bounds[a];
+        meta.boxMaxOrig[a] = bounds[3 + a];
+        // deriveTranslation (PointSource.cpp:360-366)
+        meta.translation[a] = -bounds[a];
+        meta.boxSize[a] = static_cast<float>(bounds[3 + a] + meta.translation[a]);
+    }
+    const double t[3] = {meta.translation[0], meta.translation[1], meta.translation[2]};
+    RangeReader reader = [path, info, t](uint64_t first, uint64_t count, rb_point* dst, std::string* e) {
+        return readSimlodRange(path, info, t, first, count, dst, e);
+    };
+    return std::make_unique<MemorySource>(std::move(reader), meta, batchSize ? batchSize : kSlotCapacity, device);
 }
 
 }  // namespace rbhost

@@ -72,6 +72,11 @@ public:
 std::unique_ptr<PointSource> makeMemorySource(std::vector<rb_point> points, const CloudMeta& meta,
                                               uint32_t batchSize = kSlotCapacity, int device = 0);
 
+// A .simlod file (simlod_file.h) streamed from disk batch by batch: the
+// observed box, points translated to its minimum.
+std::unique_ptr<PointSource> makeSimlodSource(const std::string& path, uint32_t batchSize, int device,
+                                              std::string* err);
+
 // The seeded synthetic lidar generator (synth.h), configuration 1, 2, 3 or 5,
 // generating each batch when the window opens for it. numPoints 0 keeps the
 // configuration's size.

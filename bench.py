@@ -242,6 +242,25 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_config5(args, world, rank, local):
+    """The full streaming run (remobench_b200/streaming.py) on each rank's GPU;
+    rank 0 prints its JSON line. Not the default step: it generates 16 GB of
+    points and takes minutes."""
+    import torch
+    from remobench_b200 import streaming
+    torch.cuda.set_device(local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    out = streaming.run(seed=1 + rank, log=lambda m: print(m, file=sys.stderr, flush=True))
+    clk = clocks.stop()
+    if rank == 0:
+        line = {"metric": "config 5 streaming: ingest Mpts/s + frame ms at 7680x4320", "value": out["ingest_mpts_s"],
+                "unit": "Mpts/s", "n_gpus": world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 points, int64/int128 sums", "data": "synthetic", "clocks": clk}
+        line.update(out)
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -253,6 +272,8 @@ def main():
     ap.add_argument("--cpu-sample-batches", type=int, default=20)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-reps", type=int, default=3)
+    ap.add_argument("--config", type=int, default=2,
+                    help="2: the benchmark (default); 5: the 1B-point full streaming run, its own JSON line")
     ap.add_argument("--no-reference-kernels", action="store_true",
                     help="reference arm: skip timing the reference's own GPU kernels")
     args = ap.parse_args()
@@ -260,6 +281,10 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+        barrier(world)
+        return
+    if args.config == 5:
+        run_config5(args, world, rank, local)
         barrier(world)
         return
 

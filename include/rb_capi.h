@@ -99,7 +99,8 @@ typedef struct rb_config {
                                         caller with its own sizing (ref_alloc's persistent size). The
                                         memory check (remolod_octree.cu:1181-1210) stops at offset +
                                         safety_margin >= store_capacity. */
-    uint32_t reserved[4];
+    uint32_t refine_voxel_capacity;  /* voxels one rb_refine_colors call can filter; 0 = 2,097,152 */
+    uint32_t reserved[3];
 } rb_config;
 
 /* CloudMeta (include/remo/PointSource.h:16-32), headless subset. */
@@ -373,6 +374,21 @@ rb_status rb_read_rollup(struct rb_ctx* ctx, uint64_t* out16, uint32_t capacity,
  * last Analysis queue are written as 1 into the node mask at mask_dev (one
  * byte per node), which rb_render takes as force_large_dev. */
 rb_status rb_refine(struct rb_ctx* ctx, uint32_t budget, uint64_t mask_dev);
+
+/* Refinement's colour filtering (wiki/02_KernelPipeline.md:232, "average
+ * colour across a node's samples"; the reference lists it, unbuilt): for the
+ * first `budget` nodes of the last Analysis queue, in queue order while their
+ * voxels fit refine_voxel_capacity, each voxel's colour becomes the mean
+ * colour of the subtree's points that fall in its cell (per 8-bit channel,
+ * rounded half up; alpha kept). The sums are kept only for the voxels being
+ * filtered, keyed by (node, cell) -- the sparse accumulator the reference's
+ * notes ask for instead of a dense per-node colour grid. */
+typedef struct rb_refine_result {
+    uint32_t nodes_filtered;   /* queue prefix taken */
+    uint32_t voxels_filtered;
+    uint64_t points_visited;   /* (point, filtered ancestor) pairs summed */
+} rb_refine_result;
+rb_status rb_refine_colors(struct rb_ctx* ctx, uint32_t budget, rb_refine_result* out);
 
 /* The learned scorer (no reference counterpart: plans/04_NeuralPass.md is
  * empty): a 16 -> 64 -> 64 -> 2 MLP, GELU, BF16 weights and activations, FP32

@@ -193,6 +193,7 @@ def lib():
         L.or_render_flat.argtypes = [vp, u64, ctypes.POINTER(Frame), vp]
         L.or_edl.argtypes = [vp, u32, u32, ctypes.c_float]
         L.or_wireframe.argtypes = [vp, ctypes.POINTER(Frame), vp, vp, u32]
+        L.or_refine_colors.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
         _lib = L
     return _lib
 
@@ -293,6 +294,13 @@ class Tree:
             return None
         g = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_uint32)), (65536,))
         return g.copy()
+
+    def refine_colors(self, nodes, capacity=2097152):
+        """Colour filtering of the nodes' voxels; (nodes filtered, voxels filtered)."""
+        arr = np.ascontiguousarray(nodes, dtype=np.uint32)
+        m, v = ctypes.c_uint32(), ctypes.c_uint64()
+        lib().or_refine_colors(self.h, _ptr(arr), len(arr), capacity, ctypes.byref(m), ctypes.byref(v))
+        return m.value, v.value
 
     def accumulate(self, batch_index):
         g = AccumGlobals()

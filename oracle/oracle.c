@@ -1257,6 +1257,119 @@ void or_render(const or_tree* t, const or_frame* f, uint64_t* fb, or_render_resu
     free(large);
 }
 
+/* ------------------------------------------------------------ Refinement */
+
+typedef struct cf_cell {
+    uint32_t cell, slot;
+} cf_cell;
+
+static int cmp_cf_cell(const void* a, const void* b) {
+    uint32_t x = ((const cf_cell*)a)->cell, y = ((const cf_cell*)b)->cell;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* The cell a voxel of n stands for, from its centre (half a cell from either
+ * boundary), with the CUDA path's float operations. */
+static uint32_t voxel_cell(const or_tree* t, const onode* n, const or_point* v) {
+    float size = t->octree_size / ldexpf(1.0f, (int)n->level);
+    float scale = 128.0f / size;
+    const uint32_t xyz[3] = {n->X, n->Y, n->Z};
+    const float pv[3] = {v->x, v->y, v->z};
+    uint32_t c[3];
+    for (int a = 0; a < 3; a++) {
+        float mn = fmaf((float)xyz[a], size, t->box_min[a]);
+        float q = floorf((pv[a] - mn) * scale);
+        int qi = (int)q;
+        c[a] = (uint32_t)(qi < 0 ? 0 : (qi > 127 ? 127 : qi));
+    }
+    return c[0] + 128u * c[1] + 16384u * c[2];
+}
+
+typedef struct cf_sums {
+    uint64_t r, g, b, n;
+} cf_sums;
+
+static void cf_add_points(const or_tree* t, const onode* leaf, uint32_t level, const cf_cell* cells, uint32_t nv,
+                          cf_sums* sums) {
+    uint32_t np = leaf->num_points, cap = leaf->num_point_chunks * t->cfg.points_per_chunk;
+    if (np > cap) np = cap;
+    const uint32_t sh = (uint32_t)OR_MAX_DEPTH + 1u - level;
+    for (uint32_t s = 0; s < np; s++) {
+        uint32_t q20[3], q28[3];
+        quantize(t, &leaf->pts[s], q20, q28);
+        uint32_t cell = ((q28[0] >> sh) & 127u) + ((q28[1] >> sh) & 127u) * 128u + ((q28[2] >> sh) & 127u) * 16384u;
+        uint32_t lo = 0, hi = nv;
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) / 2;
+            if (cells[mid].cell < cell) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo >= nv || cells[lo].cell != cell) continue;
+        cf_sums* e = &sums[cells[lo].slot];
+        uint32_t col = leaf->pts[s].color;
+        e->r += col & 255u;
+        e->g += (col >> 8) & 255u;
+        e->b += (col >> 16) & 255u;
+        e->n += 1;
+    }
+}
+
+void or_refine_colors(or_tree* t, const uint32_t* nodes, uint32_t n, uint32_t capacity, uint32_t* nodes_filtered,
+                      uint64_t* voxels_filtered) {
+    const uint32_t ppc = t->cfg.points_per_chunk;
+    uint64_t total = 0;
+    uint32_t m = 0;
+    for (; m < n; m++) {
+        const onode* nd = &t->nodes[nodes[m]];
+        uint32_t nv = nd->num_voxels, cap = nd->num_voxel_chunks * ppc;
+        if (nv > nd->num_voxels_stored) nv = nd->num_voxels_stored;
+        if (nv > cap) nv = cap;
+        if (total + nv > capacity) break;
+        total += nv;
+    }
+    uint32_t* stack = (uint32_t*)malloc((size_t)(t->num_nodes + 1) * sizeof(uint32_t));
+    if (!stack) abort();
+    for (uint32_t k = 0; k < m; k++) {
+        onode* nd = &t->nodes[nodes[k]];
+        uint32_t nv = nd->num_voxels, cap = nd->num_voxel_chunks * ppc;
+        if (nv > nd->num_voxels_stored) nv = nd->num_voxels_stored;
+        if (nv > cap) nv = cap;
+        if (nv == 0) continue;
+        cf_cell* cells = (cf_cell*)malloc((size_t)nv * sizeof(cf_cell));
+        cf_sums* sums = (cf_sums*)calloc(nv, sizeof(cf_sums));
+        if (!cells || !sums) abort();
+        for (uint32_t s = 0; s < nv; s++) {
+            cells[s].cell = voxel_cell(t, nd, &nd->vox[s]);
+            cells[s].slot = s;
+        }
+        qsort(cells, nv, sizeof(cf_cell), cmp_cf_cell);
+        /* every leaf of the subtree, the node itself if it is one */
+        uint32_t top = 0;
+        stack[top++] = nodes[k];
+        while (top) {
+            const onode* c = &t->nodes[stack[--top]];
+            if (is_leaf(c)) {
+                cf_add_points(t, c, nd->level, cells, nv, sums);
+                continue;
+            }
+            for (int q = 0; q < 8; q++)
+                if (c->child[q] >= 0) stack[top++] = (uint32_t)c->child[q];
+        }
+        for (uint32_t s = 0; s < nv; s++) {
+            if (sums[s].n == 0) continue;
+            uint64_t h = sums[s].n / 2;
+            uint32_t r = (uint32_t)((sums[s].r + h) / sums[s].n), g = (uint32_t)((sums[s].g + h) / sums[s].n),
+                     b = (uint32_t)((sums[s].b + h) / sums[s].n);
+            nd->vox[s].color = (nd->vox[s].color & 0xFF000000u) | r | (g << 8) | (b << 16);
+        }
+        free(cells);
+        free(sums);
+    }
+    free(stack);
+    *nodes_filtered = m;
+    *voxels_filtered = total;
+}
+
 /* remoClipSegment2D (remo_lines.cuh:30-55), one boundary */
 static int clip_test(float p, float q, float* t0, float* t1) {
     if (p == 0.0f) return q >= 0.0f;

@@ -223,6 +223,12 @@ void or_render(const or_tree* t, const or_frame* f, uint64_t* fb, or_render_resu
 void or_render_flat(const or_point* pts, uint64_t n, const or_frame* f, uint64_t* fb);
 /* remo_framebuffer.cuh:78-122 with libm log2f/expf in place of the intrinsics. */
 void or_edl(uint64_t* fb, uint32_t width, uint32_t height, float strength);
+/* Refinement's colour filtering (wiki/02_KernelPipeline.md:228-243): for the
+ * longest prefix of nodes[0..n) whose voxels fit capacity, each voxel's
+ * colour becomes the mean colour (per 8-bit channel, rounded half up, alpha
+ * kept) of the subtree's points in its cell. */
+void or_refine_colors(or_tree* t, const uint32_t* nodes, uint32_t n, uint32_t capacity, uint32_t* nodes_filtered,
+                      uint64_t* voxels_filtered);
 /* remoDrawListWireframe (remo_lines.cuh:120-137): the 12 box edges of each of
  * the n draw items' nodes, drawn into fb (after EDL in the reference). */
 void or_wireframe(const or_tree* t, const or_frame* f, uint64_t* fb, const uint32_t* item_nodes, uint32_t n);

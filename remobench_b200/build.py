@@ -31,6 +31,7 @@ CUDA_UNITS = {
     "rb_noalloc.cu": [],
     "rb_analysis.cu": ["-fmad=false"],
     "rb_mlp.cu": [],
+    "rb_refine.cu": ["-fmad=false"],
 }
 
 

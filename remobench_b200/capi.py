@@ -31,7 +31,7 @@ class Config(ctypes.Structure):
                 ("time_budget_ms", f32), ("voxel_mode", u32), ("accumulate", u32),
                 ("spilled_capacity", u32), ("spilling_nodes_capacity", u32), ("drawlist_capacity", u32),
                 ("safety_margin", u64), ("use_graphs", u32), ("backlog_capacity", u32),
-                ("store_capacity", u64), ("reserved", u32 * 4)]
+                ("store_capacity", u64), ("refine_voxel_capacity", u32), ("reserved", u32 * 3)]
 
 
 class CloudMeta(ctypes.Structure):
@@ -65,6 +65,10 @@ class Stats(ctypes.Structure):
                 ("nodes_split", u64), ("spilled_points", u64), ("num_grids", u32), ("overflow_flags", u32),
                 ("mem_capacity_reached", u32), ("node_capacity_reached", u32), ("num_visible_nodes", u32),
                 ("pad", u32), ("num_visible_samples", u64)]
+
+
+class RefineResult(ctypes.Structure):
+    _fields_ = [("nodes_filtered", u32), ("voxels_filtered", u32), ("points_visited", u64)]
 
 
 class RenderResult(ctypes.Structure):
@@ -139,6 +143,7 @@ SIGNATURES = {
     "rb_read_queue": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_read_rollup": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_refine": (i32, [_vp, u32, u64]),
+    "rb_refine_colors": (i32, [_vp, u32, ctypes.POINTER(RefineResult)]),
     "rb_read_features": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_mlp_init": (i32, [_vp, u64]),
     "rb_mlp_set_params": (i32, [_vp, _vp]),

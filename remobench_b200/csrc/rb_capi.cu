@@ -16,6 +16,7 @@
 #include "rb_ctx_access.h"
 #include "rb_kernels.h"
 #include "rb_mlp.h"
+#include "rb_refine.h"
 #include "rb_state.h"
 
 using rb::Counters;
@@ -29,7 +30,7 @@ enum KernelId : int {
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
     K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_PASS, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE,
-    K_EXPAND_REST, K_WIREFRAME, K_NUM
+    K_EXPAND_REST, K_WIREFRAME, K_REFINE_COLORS, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
@@ -40,7 +41,7 @@ static const char* const kKernelNames[K_NUM] = {
     "k_expand_cond", "k_zero_grids",
     // not a kernel: per-iteration expand passes run inside k_expand_rest
     "expand_pass", "k_deep_book", "k_deep_bin", "k_deep_split", "k_deep_move", "k_expand_rest",
-    "k_wireframe"};
+    "k_wireframe", "k_refine_colors"};
 
 struct Profiler {
     bool on = false;
@@ -123,6 +124,8 @@ struct rb_ctx {
     float* features = nullptr;
     float* predictions = nullptr;
     rb::MlpState mlp{};
+    rb::RefineScratch refine{};
+    rb::RefineCounters* hostRefine = nullptr;  // pinned
     bool mlpReady = false;
     uint32_t adamT = 0;
     // device-driven batches: one graph per batch, the ring descriptor it reads
@@ -393,6 +396,9 @@ void rb_release(rb_ctx* c) {
     if (c->hostRs) cudaFreeHost(c->hostRs);
     if (c->hostActr) cudaFreeHost(c->hostActr);
     c->hostActr = nullptr;
+    if (c->hostRefine) cudaFreeHost(c->hostRefine);
+    c->hostRefine = nullptr;
+    c->refine = rb::RefineScratch{};
     if (c->batchGraph) cudaGraphExecDestroy(c->batchGraph);
     c->batchGraph = nullptr;
     c->graphTried = false;
@@ -602,10 +608,26 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(c->mlp.loss, 1, "scorer loss");
     c->ingestSlots = 3;
     ALLOC(c->ingestRing, (uint64_t)c->ingestSlots * cfg.slot_capacity, "ingest ring");
+    {
+        rb::RefineScratch& r = c->refine;
+        r.capacity = cfg.refine_voxel_capacity ? cfg.refine_voxel_capacity : 2097152u;
+        r.hashMask = nextPow2(2ull * r.capacity) - 1u;
+        ALLOC(r.refSlot, N, "refinement node marks");
+        ALLOC(r.voxNode, (uint64_t)N + 1, "refinement nodes");
+        ALLOC(r.voxBase, (uint64_t)N + 1, "refinement voxel offsets");
+        ALLOC(r.acc, r.capacity, "refinement colour sums");
+        ALLOC(r.entrySlot, r.capacity, "refinement entry slots");
+        ALLOC(r.hashKeys, (uint64_t)r.hashMask + 1, "refinement cell table keys");
+        ALLOC(r.hashVals, (uint64_t)r.hashMask + 1, "refinement cell table values");
+        ALLOC(r.ctr, 1, "refinement counters");
+    }
 #undef ALLOC
     RB_CUDA(c, cudaMemsetAsync(d.hashSlots, 0xFF, (size_t)hashSize * 16, c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.ctr, 0, sizeof(Counters), c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.deepCnt, 0, (size_t)rb::kDeepRoots * rb::kDeepCells * 4, c->stream));
+    RB_CUDA(c, cudaMemsetAsync(c->refine.refSlot, 0xFF, (size_t)N * 4, c->stream));
+    RB_CUDA(c, cudaMemsetAsync(c->refine.hashKeys, 0xFF, ((size_t)c->refine.hashMask + 1) * 8, c->stream));
+    RB_CUDA(c, cudaMallocHost(&c->hostRefine, sizeof(rb::RefineCounters)));
     RB_CUDA(c, cudaMemsetAsync(d.accumGlobals, 0, sizeof(rb::AccumGlobals), c->stream));
     RB_CUDA(c, cudaMallocHost(&c->hostCtr, sizeof(Counters)));
     std::memset(c->hostCtr, 0, sizeof(Counters));
@@ -1374,6 +1396,26 @@ rb_status rb_refine(rb_ctx* c, uint32_t budget, uint64_t maskDev) {
                                                      reinterpret_cast<uint8_t*>(maskDev), c->numSMs * 2, c->stream));
     RB_CUDA(c, cudaGetLastError());
     RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return RB_OK;
+}
+
+rb_status rb_refine_colors(rb_ctx* c, uint32_t budget, rb_refine_result* out) {
+    if (!c) return RB_ERR_INVALID_ARG;
+    if (!c->analyzed) return fail(c, RB_ERR_STATE, "refine before rb_analyze");
+    if (out) std::memset(out, 0, sizeof(*out));
+    RB_CUDA(c, cudaSetDevice(c->device));
+    const uint32_t qlen = c->hostActr->queueLength;
+    LAUNCH(c, K_REFINE_COLORS, budget,
+           rb::launchRefineColors(c->d, c->refine, c->aqueue, qlen, budget, c->numSMs * 4, c->stream));
+    RB_CUDA(c, cudaGetLastError());
+    RB_CUDA(c, cudaMemcpyAsync(c->hostRefine, c->refine.ctr, sizeof(rb::RefineCounters), cudaMemcpyDeviceToHost,
+                               c->stream));
+    RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (out) {
+        out->nodes_filtered = c->hostRefine->nodes;
+        out->voxels_filtered = c->hostRefine->voxels;
+        out->points_visited = c->hostRefine->points;
+    }
     return RB_OK;
 }
 

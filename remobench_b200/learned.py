@@ -12,6 +12,12 @@
   frontier: closure-lagged (the plain method: open nodes wait for closure),
   partial (current surface variation, no learning) and learned (open nodes by
   the network's prediction of their final surface variation).
+
+A Refinement budget is a share of the frame's render time. Rasterizing is
+bound by the samples drawn, so opening a queued node costs the samples its
+children add over its own (the node's points and voxels are replaced by its
+visible children's), and a budget of f admits the queue's longest prefix whose
+added samples stay within f x the unrefined frame's samples.
 """
 import math
 
@@ -31,18 +37,18 @@ def _cloud(seed, num_points, batch):
     return cfg, pts, bmin, bmax
 
 
-SPLIT_LIMIT = 5000  # leaf split limit of the scorer experiments (deeper trees, larger frontiers)
+SPLIT_LIMIT = 50000  # leaf split limit: the reference's (remolod_structures.cuh:12)
 SV_SCALE = 300.0    # the network's output 0 is the surface-variation correction x SV_SCALE
 
 
-def collect(seeds, num_points=8 * 262144, batch=262144, closure_margin=2):
-    """(X, T, info): features of open nodes after each batch, with targets
-    (final surface variation x 3, 1 if the node gains no further points)."""
+def collect(seeds, num_points=8 * 262144, batch=262144, closure_margin=2, split_limit=SPLIT_LIMIT):
+    """(X, T): features of open nodes after each batch, with targets ((final -
+    partial) surface variation x SV_SCALE, 1 if the node gains no further points)."""
     xs, ts = [], []
     for seed in seeds:
         cfg, pts, bmin, bmax = _cloud(seed, num_points, batch)
         ctx = Context(slot_capacity=batch, time_budget_ms=0.0, max_batches_per_build=1,
-                      max_points_per_node=SPLIT_LIMIT)
+                      max_points_per_node=split_limit)
         ctx.allocate(len(pts), bmin, bmax)
         ring = DeviceRing(pts, batch, slots=ctx.cfg.ring_slots, slot_capacity=batch)
         frame = make_frame(bmin, bmax, 640, 360)
@@ -105,16 +111,38 @@ def psnr(a_rgba, b_rgba):
     return float("inf") if mse == 0 else 10.0 * math.log10(255.0 ** 2 / mse)
 
 
+def open_costs(nodes):
+    """Per node, the samples opening it adds to a frame: its children's points
+    and voxels minus its own (an upper bound: invisible children are culled)."""
+    own = nodes["num_points"].astype(np.int64) + nodes["num_voxels"].astype(np.int64)
+    kids = nodes["child"]
+    add = np.zeros(len(nodes), dtype=np.int64)
+    for c in range(8):
+        m = kids[:, c] >= 0
+        add[m] += own[kids[m, c]]
+    return np.maximum(add - own, 0)
+
+
+def budget_prefix(queue, costs, allowance):
+    """The longest prefix of `queue` whose summed costs stay within allowance."""
+    if len(queue) == 0:
+        return 0
+    csum = np.cumsum(costs[queue])
+    return int(np.searchsorted(csum, allowance, side="right"))
+
+
 def evaluate(params, seed, num_points=8 * 262144, batch=262144, stop_batch=None, closure_margin=2,
-             fractions=(0.05, 0.10, 0.20, 0.40), views=3, width=960, height=540, budget_px=64.0):
-    """PSNR versus flat for each ranking and budget, averaged over `views`
-    orbit frames, on the tree after `stop_batch` batches of a held-out cloud."""
+             fractions=(0.05, 0.10, 0.20, 0.40), views=3, width=960, height=540, budget_px=64.0,
+             split_limit=SPLIT_LIMIT):
+    """PSNR versus flat for each ranking and budget (a share of the frame's
+    render time, see the module notes), averaged over `views` orbit frames, on
+    the tree after `stop_batch` batches of a held-out cloud."""
     import torch
     cfg, pts, bmin, bmax = _cloud(seed, num_points, batch)
     nb = (len(pts) + batch - 1) // batch
     stop = nb // 2 if stop_batch is None else stop_batch
     ctx = Context(slot_capacity=batch, time_budget_ms=0.0, max_batches_per_build=1,
-                  max_points_per_node=SPLIT_LIMIT)
+                  max_points_per_node=split_limit)
     ctx.allocate(len(pts), bmin, bmax)
     ring = DeviceRing(pts, batch, slots=ctx.cfg.ring_slots, slot_capacity=batch)
     consumed = 0
@@ -126,7 +154,9 @@ def evaluate(params, seed, num_points=8 * 262144, batch=262144, stop_batch=None,
     flat_ctx = Context(pipeline=capi.RB_PIPELINE_FLAT)
     flat_ctx.allocate(len(pts), bmin, bmax)
     ingested = torch.from_numpy(pts[:consumed * batch].view(np.float32).reshape(-1, 4)).cuda()
-    nn = len(ctx.nodes())
+    nodes = ctx.nodes()
+    nn = len(nodes)
+    costs = open_costs(nodes)
     mask = torch.zeros(nn, dtype=torch.uint8, device="cuda")
     fb = torch.empty(width * height, dtype=torch.int64, device="cuda")
     rgba = torch.empty(width * height, dtype=torch.int32, device="cuda")
@@ -136,29 +166,34 @@ def evaluate(params, seed, num_points=8 * 262144, batch=262144, stop_batch=None,
     out = {m: {f: [] for f in fractions} for m in modes}
     out["none"] = []
     path = orbit_path(bmin, bmax, views, seed=seed + 1000)
+    frontiers, admitted = [], {m: {f: [] for f in fractions} for m in modes}
     for (yaw, pitch, rs) in path:
         frame = make_frame(bmin, bmax, width, height, yaw=yaw, pitch=pitch, radius_scale=rs, budget=budget_px)
         flat_ctx.render_flat(frame, ingested, fb, rgba)
         truth = rgba.cpu().numpy().copy()
-        ctx.render(frame, fb, rgba)
+        base = ctx.render(frame, fb, rgba)
         out["none"].append(psnr(rgba.cpu().numpy(), truth))
-        # the frontier Refinement can open, from the partial ranking's eligibility
+        # the frontier Refinement can open
         ctx.analyze(frame, min_points=MIN_POINTS, closure_margin=closure_margin, score_mode=capi.RB_SCORE_PARTIAL,
                     queue_capacity=16384)
         a = ctx.analysis()
-        frontier = int(np.sum(((a["flags"] & 4) != 0) & (a["count"] >= MIN_POINTS)))
+        frontiers.append(int(np.sum(((a["flags"] & 4) != 0) & (a["count"] >= MIN_POINTS))))
         for name, mode in modes.items():
             ctx.analyze(frame, min_points=MIN_POINTS, closure_margin=closure_margin, score_mode=mode,
                         queue_capacity=16384)
+            queue = ctx.queue()
             for f in fractions:
-                k = int(round(f * frontier))
+                k = budget_prefix(queue, costs, f * base.draw_samples)
+                admitted[name][f].append(k)
                 ctx.refine(k, mask)
                 ctx.render(frame, fb, rgba, force_large=mask)
                 out[name][f].append(psnr(rgba.cpu().numpy(), truth))
+    frontier = float(np.mean(frontiers))
     result = {"seed": seed, "stop_batch": stop, "points": consumed * batch, "nodes": nn, "frontier": frontier,
               "psnr_none": float(np.mean(out["none"]))}
     for name in modes:
         result[name] = {f"{int(f * 100)}%": float(np.mean(out[name][f])) for f in fractions}
+        result[name + "_nodes"] = {f"{int(f * 100)}%": float(np.mean(admitted[name][f])) for f in fractions}
     ctx.close()
     flat_ctx.close()
     return result
@@ -180,13 +215,14 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=262144)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--margin", type=int, default=2)
+    ap.add_argument("--split-limit", type=int, default=SPLIT_LIMIT)
     ap.add_argument("--save", default=None, help="write the trained parameters (.npy)")
     args = ap.parse_args(argv)
     t0 = time.time()
     train_seeds = list(range(100, 100 + args.train_seeds))
     eval_seeds = list(range(900, 900 + args.eval_seeds))
-    X, T = collect(train_seeds, args.points, args.batch, args.margin)
-    Xv, Tv = collect(eval_seeds, args.points, args.batch, args.margin)
+    X, T = collect(train_seeds, args.points, args.batch, args.margin, args.split_limit)
+    Xv, Tv = collect(eval_seeds, args.points, args.batch, args.margin, args.split_limit)
     t_collect = time.time() - t0
     cfg, _, bmin, bmax = _cloud(1, args.batch, args.batch)
     ctx = Context(slot_capacity=args.batch)
@@ -201,11 +237,14 @@ def main(argv=None):
     sv_err_learned = float(np.mean(np.abs(pv[:, 0] - Tv[:, 0]) / SV_SCALE))
     sv_err_partial = float(np.mean(np.abs(Tv[:, 0]) / SV_SCALE))
     closure_acc = float(np.mean((pv[:, 1] > 0) == (Tv[:, 1] > 0.5)))
-    evals = [evaluate(params, s, args.points, args.batch, closure_margin=args.margin) for s in eval_seeds]
+    evals = [evaluate(params, s, args.points, args.batch, closure_margin=args.margin, split_limit=args.split_limit)
+             for s in eval_seeds]
     frontier = float(np.mean([e["frontier"] for e in evals]))
     summary = {}
     for mode in ("closure_lagged", "partial", "learned"):
         summary[mode] = {k: float(np.mean([e[mode][k] for e in evals])) for k in evals[0][mode]}
+        summary[mode + "_nodes"] = {k: float(np.mean([e[mode + "_nodes"][k] for e in evals]))
+                                    for k in evals[0][mode + "_nodes"]}
     print(json.dumps({"train_pairs": int(len(X)), "heldout_pairs": int(len(Xv)), "final_train_loss": hist[-1],
                       "heldout_sv_mae_learned": sv_err_learned, "heldout_sv_mae_partial": sv_err_partial,
                       "heldout_closure_accuracy": closure_acc, "psnr_no_refinement": float(np.mean([e["psnr_none"] for e in evals])),

@@ -247,6 +247,12 @@ class Context:
     def refine(self, budget, mask):
         self._ok(capi.lib().rb_refine(self.h, int(budget), mask.data_ptr()))
 
+    def refine_colors(self, budget):
+        """Colour filtering of the first `budget` queued nodes' voxels (rb_refine_colors)."""
+        r = capi.RefineResult()
+        self._ok(capi.lib().rb_refine_colors(self.h, int(budget), ctypes.byref(r)))
+        return r
+
     def set_stream(self, stream_handle):
         self._ok(capi.lib().rb_set_stream(self.h, ctypes.c_void_p(int(stream_handle))))
 

@@ -126,3 +126,37 @@ def test_refine_mask_marks_queue_prefix(analysed):
     m = mask.cpu().numpy()
     assert set(np.nonzero(m)[0].tolist()) == set(q[:budget].tolist())
     assert np.all(m[m != 0] == 1)
+
+
+def test_colour_filtering_matches_oracle_and_lifts_psnr(c1_cloud):
+    """Refinement's colour filtering (rb_refine_colors) on the queue's first
+    nodes: every voxel colour equals the oracle's filtered colour (integer
+    means, order-independent), the capacity admits a queue prefix, and the
+    filtered frame is closer to the flat render than the unfiltered one."""
+    import torch
+    from gpu_helpers import compare_voxels
+    from remobench_b200 import capi, quality
+    from remobench_b200.lod import Context, make_frame
+    cfg, cloud, bmin, bmax = c1_cloud
+    ctx, _ = build_gpu(cloud, bmin, bmax, cfg.batch_size, refine_voxel_capacity=400000)
+    tree = build_oracle(cloud, bmin, bmax, cfg.batch_size)
+    f = make_frame(bmin, bmax, W, H, yaw=1.3, pitch=-0.5, radius_scale=0.5, budget=64.0)
+    flat = Context(pipeline=capi.RB_PIPELINE_FLAT)
+    flat.allocate(len(cloud), bmin, bmax)
+    dev = torch.from_numpy(cloud.view(np.float32).reshape(-1, 4)).cuda()
+    before = quality.compare(ctx, flat, dev, f)["psnr"]
+    ctx.analyze(f, frontier_only=False, queue_capacity=4096)
+    queue = ctx.queue()
+    assert len(queue) > 50
+    r = ctx.refine_colors(len(queue))
+    m, nv = tree.refine_colors(queue, capacity=400000)
+    assert (r.nodes_filtered, r.voxels_filtered) == (m, nv)
+    assert 0 < r.nodes_filtered <= len(queue)
+    assert r.points_visited > 0
+    compare_voxels(ctx, tree, ctx.nodes())
+    after = quality.compare(ctx, flat, dev, f)["psnr"]
+    assert after > before, (before, after)
+    # a second call on the same queue (no new points) leaves the colours alone
+    r2 = ctx.refine_colors(len(queue))
+    assert r2.voxels_filtered == r.voxels_filtered
+    compare_voxels(ctx, tree, ctx.nodes())

@@ -228,3 +228,25 @@ def test_threaded_builder_matches_sequential(c1_cloud):
         pb, ib = b.leaf_points(i)
         assert np.array_equal(ia, ib) and np.array_equal(pa.view(np.uint32), pb.view(np.uint32))
         assert np.array_equal(a.node_voxels(i).view(np.uint32), b.node_voxels(i).view(np.uint32))
+
+
+def test_colour_filtering_known_answer():
+    # five points in one root cell (128^3 grid of a unit cube) split the root
+    # (limit 4); the root keeps one voxel for the cell, coloured by the lowest
+    # index; filtering makes it the mean of the five points, rounded half up
+    t = unit_tree(max_points_per_node=4)
+    cols = [(10, 20, 30), (20, 30, 40), (30, 40, 51), (40, 50, 60), (51, 60, 70)]
+    cloud = pts([(0.3 + 0.0005 * i, 0.6, 0.6, r | (g << 8) | (b << 16) | (200 << 24))
+                 for i, (r, g, b) in enumerate(cols)])
+    t.add_batch(cloud)
+    t.sweep()
+    assert not t.node(0).is_leaf
+    v = t.node_voxels(0)
+    assert len(v) == 1 and int(v[0]["color"]) == int(cloud[0]["color"])
+    m, nv = t.refine_colors([0])
+    assert (m, nv) == (1, 1)
+    c = int(t.node_voxels(0)[0]["color"])
+    mean = [(sum(x[k] for x in cols) + 2) // 5 for k in range(3)]
+    assert (c & 255, (c >> 8) & 255, (c >> 16) & 255, c >> 24) == (mean[0], mean[1], mean[2], 200)
+    # a capacity below the node's voxels filters nothing
+    assert t.refine_colors([0], capacity=0) == (0, 0)

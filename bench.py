@@ -160,6 +160,32 @@ def sample_identity(pts, sample_batches):
     return {"first_batch": 0, "batches": sample_batches, "points": int(n), "blake2b_64": h}
 
 
+def ncu_traffic(kernel):
+    """The kernel's DRAM traffic per 1M-point launch from the committed ncu
+    capture summary (profiles/ncu_traffic.json, written from an ncu capture of
+    the build it names), or None with the reason when there is none or the
+    kernel's source changed since the capture."""
+    import hashlib
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            table = json.load(f)
+    except Exception:
+        return None, "no ncu capture summary"
+    row = table.get("kernels", {}).get(kernel)
+    if row is None:
+        return None, f"no ncu capture of {kernel}"
+    src = os.path.join(ROOT, row["source"])
+    try:
+        with open(src, "rb") as f:
+            digest = hashlib.sha256(f.read()).hexdigest()[:16]
+    except Exception:
+        return None, f"{row['source']} missing"
+    if digest != row["source_sha256_16"]:
+        return None, f"{row['source']} changed since the capture ({row['captured']})"
+    return row["dram_bytes_per_launch"], f"ncu capture {row['captured']}: {row['workload']}"
+
+
 def cpu_baseline(pts, bmin, bmax, sample_batches, threads):
     """The oracle (CPU restatement of the reference's builder) on the first
     sample_batches batches of the same cloud: Update + Accumulate."""
@@ -405,25 +431,38 @@ def main():
     upd = {k: v for k, v in prof.items() if v["timed"] > 0 and k not in ("k_reset_root",)}
     total_k = sum(v["ms"] for v in upd.values())
     top = max(upd.items(), key=lambda kv: kv[1]["ms"])
-    # algorithmic bytes of the dominant kernel per point handed to it: the point
+    # algorithmic bytes of a kernel per unit handed to it (points): the point
     # read (16 B), plus its leaf id (4 B) where one is written, plus the stored
     # point and index (20 B) for insertion
     bytes_per_unit = {"k_vox_sample": 16.0, "k_count_first": 20.0, "k_insert": 16.0 + 4.0 + 20.0,
-                      "k_recount": 4.0, "k_accumulate": 16.0}
-    # DRAM bytes (read + write) per launch from one ncu capture of the kernel on
-    # 1M-point batches of the same generator (profiles/k_vox_sample_config2_1M_batch.md)
-    ncu_traffic = {"k_vox_sample": 43.1e6}
+                      "k_recount": 4.0, "k_accumulate": 16.0, "k_deep_bin": 4.0, "k_deep_move": 4.0}
     peak, peak_kind = peaks()
     roof = None
     if top[0] in bytes_per_unit and top[1]["units"] > 0:
         avg_ms = top[1]["ms"] / top[1]["timed"]
         per_launch_bytes = bytes_per_unit[top[0]] * top[1]["units"] / top[1]["launches"]
         achieved = per_launch_bytes / (avg_ms / 1e3) / 1e9
+        traffic, traffic_note = ncu_traffic(top[0])
         roof = {"bound": "hbm", "kernel": top[0], "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 5), "peak_kind": peak_kind,
-                "traffic": ncu_traffic.get(top[0]), "traffic_unit": "bytes per launch (ncu)",
+                "traffic": traffic, "traffic_unit": "DRAM bytes read + written per launch (ncu)",
+                "traffic_source": traffic_note,
                 "algorithmic_bytes_per_launch": round(per_launch_bytes),
                 "avg_launch_ms": round(avg_ms, 4), "share": round(top[1]["ms"] / total_k, 3)}
+
+    # the raster against the same HBM peak: per frame, clearing the packed
+    # framebuffer (8 B/px), reading every drawn sample (16 B) and its 64-bit
+    # atomicMin (8 B), EDL reading and writing each pixel (16 B/px) and the
+    # resolve reading the packed and writing the RGBA pixel (12 B/px)
+    raster_roof = None
+    if frame_ms:
+        p50_ms = float(np.percentile(frame_ms, 50))
+        px = WIDTH * HEIGHT
+        frame_bytes = px * (8 + 16 + 12) + float(np.median(samples)) * (16 + 8)
+        ach = frame_bytes / (p50_ms / 1e3) / 1e9
+        raster_roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                       "frac": round(ach / peak, 4), "peak_kind": peak_kind,
+                       "algorithmic_bytes_per_frame": round(frame_bytes), "p50_ms": round(p50_ms, 4)}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample_batches > 0:
@@ -454,6 +493,7 @@ def main():
                      "max_depth": stats.max_depth, "spilled": stats.spilled_points},
             "gpu_launches": int(launches),
             "roofline": roof,
+            "raster_roofline": raster_roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk,

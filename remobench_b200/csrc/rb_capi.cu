@@ -281,13 +281,14 @@ bool graphPath(rb_ctx* c) {
     return c->batchGraph != nullptr;
 }
 
-// Launches of graph batches, for the per-kernel counts: fourteen kernels per
-// batch; the per-iteration passes k_expand_rest ran (one loop test each) are
-// counted as expand_pass, not as launches.
+// Launches of graph batches, for the per-kernel counts: thirteen kernels per
+// batch (k_expand_rest zeroes the split grids); the per-iteration passes
+// k_expand_rest ran (one loop test each) are counted as expand_pass, not as
+// launches.
 void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint64_t points) {
     const uint32_t passes = c->hostCtr->condRuns - condBefore;
     for (int k : {K_BATCH_BEGIN, K_COUNT_FIRST, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE, K_EXPAND_REST,
-                  K_ZERO_GRIDS, K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END})
+                  K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_CHUNKS, K_INSERT, K_VOX_STORE, K_BATCH_END})
         c->prof.launches[k] += batches;
     c->prof.launches[K_EXPAND_PASS] += passes;
     for (int k : {K_COUNT_FIRST, K_DEEP_BIN, K_DEEP_MOVE, K_VOX_SAMPLE, K_INSERT}) c->prof.units[k] += points;

@@ -1246,6 +1246,33 @@ __global__ void __launch_bounds__(256) k_deep_move(Dev d, const Point* __restric
     }
 }
 
+// The grids of the nodes split in this batch (zeroed at every split,
+// :372-387) and the expand round's bins, cleared once after the expand loop
+// (nothing reads a split grid before voxel sampling). Work items of 16 KB
+// spread over every block of the caller's grid.
+__device__ void zeroGridsBody(const Dev& d) {
+    const Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t nz = c->numZero < d.zeroCap ? c->numZero : d.zeroCap;
+    constexpr uint32_t kPiece = 1024;  // uint4 per work item
+    constexpr uint32_t kPieces = kGridWords / 4u / kPiece;
+    const uint32_t deepUnits = (c->deepRoots * kDeepCells + 3u) / 4u;  // rows are contiguous from slot 0
+    const uint32_t deepItems = (deepUnits + kPiece - 1u) / kPiece;
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    for (uint32_t w = blockIdx.x; w < nz * kPieces + deepItems; w += gridDim.x) {
+        if (w < nz * kPieces) {
+            uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, d.zeroList[w / kPieces])) + (w % kPieces) * kPiece;
+            for (uint32_t q = threadIdx.x; q < kPiece; q += blockDim.x) g[q] = z;
+        } else {
+            const uint32_t u0 = (w - nz * kPieces) * kPiece;
+            uint4* g = reinterpret_cast<uint4*>(d.deepCnt);
+            for (uint32_t q = u0 + threadIdx.x; q < u0 + kPiece && q < deepUnits; q += blockDim.x) g[q] = z;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_zero_grids(Dev d) { zeroGridsBody(d); }
+
 // Grid-wide barrier of a cooperative launch. Every block is resident, so the
 // wait ends once each block arrives; the polls are still bounded (about a
 // second), after which the block records kOvfSync, the others stop waiting
@@ -1285,51 +1312,30 @@ __device__ bool gridBarrier(Counters* c, uint32_t& epoch) {
 // batch the expand round left unfinished -- nodes still over the limit at its
 // deepest binned level, or a first count it did not take -- as one
 // cooperative kernel with grid barriers between the phases, so the batch
-// graph needs no conditional node. Most batches return at once: the round
-// left nothing to split. Launched with one 1024-thread block per SM.
+// graph needs no conditional node; then the batch's split grids are zeroed
+// (zeroGridsBody), which saves the graph a node. Most batches only zero: the
+// round left nothing to split. Launched with one 1024-thread block per SM.
 __global__ void __launch_bounds__(1024, 1) k_expand_rest(Dev d) {
     Counters* c = d.ctr;
-    // no block writes these before the first barrier: every block decides alike
-    if (c->batchStop || c->numSpill == 0u) return;
-    uint32_t epoch = 0;
-    for (uint32_t pass = 0; pass < 64u; pass++) {
-        if (!gridBarrier(c, epoch)) return;
-        if (blockIdx.x == 0) splitBody(d, 0u, 0u);
-        if (!gridBarrier(c, epoch)) return;
-        spillCopyBody(d, 0u);
-        if (!gridBarrier(c, epoch)) return;
-        recountBody(d, nullptr, 0u, 0u, 0u);
-        if (!gridBarrier(c, epoch)) return;
-        if (blockIdx.x == 0) expandCondBody(d, 0ull, 0u);
-        if (!gridBarrier(c, epoch)) return;
-        // the next pass's split comes after its first barrier: all read alike
-        if (c->loopMore == 0u) return;
-    }
-}
-
-// The grids of the nodes split in this batch (zeroed at every split,
-// :372-387) and the expand round's bins, cleared once after the expand loop
-// (nothing reads a split grid before voxel sampling). Work items of 16 KB
-// spread over every block.
-__global__ void __launch_bounds__(256) k_zero_grids(Dev d) {
-    const Counters* c = d.ctr;
     if (c->batchStop) return;
-    const uint32_t nz = c->numZero < d.zeroCap ? c->numZero : d.zeroCap;
-    constexpr uint32_t kPiece = 1024;  // uint4 per work item
-    constexpr uint32_t kPieces = kGridWords / 4u / kPiece;
-    const uint32_t deepUnits = (c->deepRoots * kDeepCells + 3u) / 4u;  // rows are contiguous from slot 0
-    const uint32_t deepItems = (deepUnits + kPiece - 1u) / kPiece;
-    const uint4 z = make_uint4(0, 0, 0, 0);
-    for (uint32_t w = blockIdx.x; w < nz * kPieces + deepItems; w += gridDim.x) {
-        if (w < nz * kPieces) {
-            uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, d.zeroList[w / kPieces])) + (w % kPieces) * kPiece;
-            for (uint32_t q = threadIdx.x; q < kPiece; q += blockDim.x) g[q] = z;
-        } else {
-            const uint32_t u0 = (w - nz * kPieces) * kPiece;
-            uint4* g = reinterpret_cast<uint4*>(d.deepCnt);
-            for (uint32_t q = u0 + threadIdx.x; q < u0 + kPiece && q < deepUnits; q += blockDim.x) g[q] = z;
+    // no block writes numSpill before the first barrier: every block decides alike
+    if (c->numSpill != 0u) {
+        uint32_t epoch = 0;
+        for (uint32_t pass = 0; pass < 64u; pass++) {
+            if (!gridBarrier(c, epoch)) return;
+            if (blockIdx.x == 0) splitBody(d, 0u, 0u);
+            if (!gridBarrier(c, epoch)) return;
+            spillCopyBody(d, 0u);
+            if (!gridBarrier(c, epoch)) return;
+            recountBody(d, nullptr, 0u, 0u, 0u);
+            if (!gridBarrier(c, epoch)) return;
+            if (blockIdx.x == 0) expandCondBody(d, 0ull, 0u);
+            if (!gridBarrier(c, epoch)) return;
+            // the next pass's split comes after its first barrier: all read alike
+            if (c->loopMore == 0u) break;
         }
     }
+    zeroGridsBody(d);
 }
 
 __device__ __forceinline__ uint32_t hashSlot(unsigned long long key, uint32_t mask) {
@@ -2073,7 +2079,6 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int re
         k_deep_split<<<1, 1024, 0, cs>>>(d);
         k_deep_move<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         if ((e = launchExpandRest(d, restGrid, cs)) != cudaSuccess) break;
-        k_zero_grids<<<fixedGrid, 256, 0, cs>>>(d);
         k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         k_vox_commit<<<fixedGrid, 256, 0, cs>>>(d);
         k_alloc_chunks<<<fixedGrid, 256, 0, cs>>>(d);

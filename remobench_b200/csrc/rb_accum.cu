@@ -35,6 +35,30 @@ __device__ __forceinline__ unsigned long long mortonSpread(uint32_t v) {
     return x;
 }
 
+// The watermark is the largest 60-bit Morton code of the folded points.
+// Codes are compared without building them: the dimension whose coordinates
+// differ in the highest bit decides (x before y before z at the same bit, the
+// order of the interleave), found with the test "msb(p) < msb(q)" =
+// p < q && p < (p ^ q) (Chan, "Closest-point problems simplified on the RAM",
+// SODA 2002). Only the block's largest point is spread into a code.
+__device__ __forceinline__ bool msbLess(uint32_t p, uint32_t q) { return p < q && p < (p ^ q); }
+
+__device__ __forceinline__ bool mortonLess(uint32_t ax, uint32_t ay, uint32_t az, uint32_t bx, uint32_t by,
+                                           uint32_t bz) {
+    const uint32_t dx = ax ^ bx, dy = ay ^ by, dz = az ^ bz;
+    uint32_t da = dx, a = ax, b = bx;
+    if (msbLess(da, dy)) {
+        da = dy;
+        a = ay;
+        b = by;
+    }
+    if (msbLess(da, dz)) {
+        a = az;
+        b = bz;
+    }
+    return a < b;
+}
+
 __device__ __forceinline__ void add128(unsigned long long& lo, unsigned long long& hi,
                                        unsigned long long v) {
     const unsigned long long o = lo;
@@ -185,7 +209,7 @@ __global__ void __launch_bounds__(kAccumThreads, 4) k_accumulate(Dev d, uint32_t
         unsigned long long s1[3] = {0, 0, 0};
         unsigned long long p2[6] = {0, 0, 0, 0, 0, 0};
         uint32_t c1[3] = {0, 0, 0}, c2[3] = {0, 0, 0};
-        unsigned long long wm = 0;
+        uint32_t mx = 0, my = 0, mz = 0;  // the largest point in Morton order so far
         for (uint32_t s0 = from + threadIdx.x; s0 < end; s0 += 2u * blockDim.x) {
             // two points per step: independent chunk-table and point loads in flight
             float4 v2[2];
@@ -209,18 +233,20 @@ __global__ void __launch_bounds__(kAccumThreads, 4) k_accumulate(Dev d, uint32_t
                 const uint32_t P[3] = {aq(v.x, d.boxMin[0], d.octreeSize, 268435456.0f),
                                        aq(v.y, d.boxMin[1], d.octreeSize, 268435456.0f),
                                        aq(v.z, d.boxMin[2], d.octreeSize, 268435456.0f)};
-                long long q[3] = {(long long)P[0] - bx, (long long)P[1] - by, (long long)P[2] - bz};
+                // clamped to [0, 2^(28 - level)]: 32-bit values, 64-bit products
+                uint32_t q[3];
+                const long long r[3] = {(long long)P[0] - bx, (long long)P[1] - by, (long long)P[2] - bz};
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    q[k] = q[k] < 0 ? 0 : (q[k] > lim ? lim : q[k]);
-                    s1[k] += (unsigned long long)q[k];
+                    q[k] = (uint32_t)(r[k] < 0 ? 0 : (r[k] > lim ? lim : r[k]));
+                    s1[k] += q[k];
                 }
-                p2[0] += (unsigned long long)(q[0] * q[0]);
-                p2[1] += (unsigned long long)(q[0] * q[1]);
-                p2[2] += (unsigned long long)(q[0] * q[2]);
-                p2[3] += (unsigned long long)(q[1] * q[1]);
-                p2[4] += (unsigned long long)(q[1] * q[2]);
-                p2[5] += (unsigned long long)(q[2] * q[2]);
+                p2[0] += (unsigned long long)q[0] * q[0];
+                p2[1] += (unsigned long long)q[0] * q[1];
+                p2[2] += (unsigned long long)q[0] * q[2];
+                p2[3] += (unsigned long long)q[1] * q[1];
+                p2[4] += (unsigned long long)q[1] * q[2];
+                p2[5] += (unsigned long long)q[2] * q[2];
                 const uint32_t col = __float_as_uint(v.w);
                 const uint32_t ch[3] = {col & 255u, (col >> 8) & 255u, (col >> 16) & 255u};
 #pragma unroll
@@ -236,10 +262,14 @@ __global__ void __launch_bounds__(kAccumThreads, 4) k_accumulate(Dev d, uint32_t
                 X = X < 1048575u ? X : 1048575u;
                 Y = Y < 1048575u ? Y : 1048575u;
                 Z = Z < 1048575u ? Z : 1048575u;
-                const unsigned long long m = (mortonSpread(X) << 2) | (mortonSpread(Y) << 1) | mortonSpread(Z);
-                wm = m > wm ? m : wm;
+                if (mortonLess(mx, my, mz, X, Y, Z)) {
+                    mx = X;
+                    my = Y;
+                    mz = Z;
+                }
             }
         }
+        unsigned long long wm = (mortonSpread(mx) << 2) | (mortonSpread(my) << 1) | mortonSpread(mz);
         unsigned long long lo2[6], hi2[6] = {0, 0, 0, 0, 0, 0};
         unsigned long long c1w[3], c2w[3];
 #pragma unroll

@@ -39,6 +39,7 @@ def _cloud(seed, num_points, batch):
 
 SPLIT_LIMIT = 50000  # leaf split limit: the reference's (remolod_structures.cuh:12)
 SV_SCALE = 300.0    # the network's output 0 is the surface-variation correction x SV_SCALE
+OFF_W3, OFF_B3 = 5248, 5376  # W3 [2][64] and b3 [2] in the parameter vector (include/rb_capi.h)
 
 
 def collect(seeds, num_points=8 * 262144, batch=262144, closure_margin=2, split_limit=SPLIT_LIMIT):
@@ -102,6 +103,22 @@ def predict(ctx, X):
     y = torch.empty((len(X), 2), dtype=torch.float32, device="cuda")
     ctx.mlp_predict(xd, y)
     return y.cpu().numpy()
+
+
+def calibrate(ctx, Xval, Tval):
+    """Shrinks the predicted correction toward none by the factor that best fits
+    a validation split (least squares on output 0, clipped to [0, 1]), folded
+    into the output layer's first row and bias, so the scorer never trusts its
+    correction more than held-out data supports. Returns the factor."""
+    y = predict(ctx, Xval)[:, 0].astype(np.float64)
+    t = Tval[:, 0].astype(np.float64)
+    den = float(np.dot(y, y))
+    alpha = 0.0 if den <= 0.0 else float(np.clip(np.dot(y, t) / den, 0.0, 1.0))
+    p = ctx.mlp_params().copy()
+    p[OFF_W3:OFF_W3 + 64] *= alpha  # W3 row 0
+    p[OFF_B3] *= alpha              # b3[0]
+    ctx.mlp_set_params(p)
+    return alpha
 
 
 def psnr(a_rgba, b_rgba):
@@ -228,7 +245,10 @@ def main(argv=None):
     ctx = Context(slot_capacity=args.batch)
     ctx.allocate(args.batch, bmin, bmax)
     ctx.mlp_init(1)
-    hist = train(ctx, X, T, epochs=args.epochs)
+    # the last eighth of the training seeds' pairs validates the calibration
+    nval = max(1, len(X) // 8)
+    hist = train(ctx, X[:-nval], T[:-nval], epochs=args.epochs)
+    alpha = calibrate(ctx, X[-nval:], T[-nval:])
     params = ctx.mlp_params()
     if args.save:
         np.save(args.save, params)
@@ -246,6 +266,7 @@ def main(argv=None):
         summary[mode + "_nodes"] = {k: float(np.mean([e[mode + "_nodes"][k] for e in evals]))
                                     for k in evals[0][mode + "_nodes"]}
     print(json.dumps({"train_pairs": int(len(X)), "heldout_pairs": int(len(Xv)), "final_train_loss": hist[-1],
+                      "calibration": alpha,
                       "heldout_sv_mae_learned": sv_err_learned, "heldout_sv_mae_partial": sv_err_partial,
                       "heldout_closure_accuracy": closure_acc, "psnr_no_refinement": float(np.mean([e["psnr_none"] for e in evals])),
                       "psnr": summary, "frontier_nodes": frontier, "collect_s": round(t_collect, 1),

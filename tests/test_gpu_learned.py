@@ -34,7 +34,10 @@ def trained():
     ctx = Context(slot_capacity=262144)
     ctx.allocate(262144, bmin, bmax)
     ctx.mlp_init(1)
-    hist = learned.train(ctx, X, T, epochs=30)
+    nval = len(X) // 8
+    hist = learned.train(ctx, X[:-nval], T[:-nval], epochs=30)
+    alpha = learned.calibrate(ctx, X[-nval:], T[-nval:])
+    assert 0.0 <= alpha <= 1.0
     return ctx.mlp_params(), hist, len(X)
 
 

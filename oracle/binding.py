@@ -193,6 +193,7 @@ def lib():
         L.or_render_flat.argtypes = [vp, u64, ctypes.POINTER(Frame), vp]
         L.or_edl.argtypes = [vp, u32, u32, ctypes.c_float]
         L.or_wireframe.argtypes = [vp, ctypes.POINTER(Frame), vp, vp, u32]
+        L.or_features.argtypes = [vp, u32, u32, vp]
         L.or_refine_colors.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
         _lib = L
     return _lib
@@ -294,6 +295,12 @@ class Tree:
             return None
         g = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_uint32)), (65536,))
         return g.copy()
+
+    def features(self, current_batch, closure_margin):
+        """(num_nodes, 16) float32: the learned scorer's inputs per node."""
+        out = np.zeros((self.num_nodes(), 16), dtype=np.float32)
+        lib().or_features(self.h, current_batch, closure_margin, _ptr(out))
+        return out
 
     def refine_colors(self, nodes, capacity=2097152):
         """Colour filtering of the nodes' voxels; (nodes filtered, voxels filtered)."""

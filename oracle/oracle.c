@@ -959,6 +959,77 @@ void or_analyze_fp64(const or_tree* t, or_analysis_node* out) {
     free(all);
 }
 
+/* The learned scorer's 16 inputs per node, as rb_analyze logs them: log
+ * count, level, mean, normalised centred second moments, surface variation and
+ * planarity (from the FP64 eigen-solve here), fill, colour variance, age. */
+void or_features(const or_tree* t, uint32_t current_batch, uint32_t closure_margin, float* out16) {
+    const uint32_t nn = t->num_nodes;
+    uint64_t* sums = (uint64_t*)calloc((size_t)(nn ? nn : 1) * 16, sizeof(uint64_t));
+    uint32_t* lt = (uint32_t*)calloc(nn ? nn : 1, sizeof(uint32_t));
+    uint64_t* col = (uint64_t*)calloc((size_t)(nn ? nn : 1) * 6, sizeof(uint64_t));
+    or_analysis_node* eig = (or_analysis_node*)calloc(nn ? nn : 1, sizeof(or_analysis_node));
+    if (!sums || !lt || !col || !eig) abort();
+    or_rolled_sums(t, sums, lt);
+    or_analyze_fp64(t, eig);
+    /* colour sums roll up unchanged: children have larger ids than their parent */
+    for (uint32_t k = nn; k-- > 0;) {
+        const onode* n = &t->nodes[k];
+        uint64_t* c = col + (size_t)k * 6;
+        if (is_leaf(n)) {
+            for (int a = 0; a < 3; a++) {
+                c[a] = n->ai.c1[a];
+                c[3 + a] = n->ai.c2[a];
+            }
+        } else {
+            for (int q = 0; q < 8; q++) {
+                if (n->child[q] < 0) continue;
+                const uint64_t* cc = col + (size_t)n->child[q] * 6;
+                for (int a = 0; a < 6; a++) c[a] += cc[a];
+            }
+        }
+    }
+    const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 2};
+    for (uint32_t i = 0; i < nn; i++) {
+        const onode* n = &t->nodes[i];
+        const uint64_t* r = sums + (size_t)i * 16;
+        const uint64_t cnt = r[0];
+        float* ft = out16 + (size_t)i * 16;
+        const double nd = cnt ? (double)cnt : 1.0;
+        const double unit = ldexp(1.0, (int)(28u - n->level));
+        ft[0] = log2f(1.0f + (float)cnt) * (1.0f / 24.0f);
+        ft[1] = (float)n->level * (1.0f / 20.0f);
+        for (int k = 0; k < 3; k++) ft[2 + k] = cnt ? (float)((double)r[1 + k] / (nd * unit)) : 0.0f;
+        for (int k = 0; k < 6; k++) {
+            float v = 0.0f;
+            if (cnt >= 2) {
+                const u128 s2 = ((u128)r[4 + 2 * k + 1] << 64) | r[4 + 2 * k];
+                const i128 c = (i128)((u128)cnt * s2) - (i128)r[1 + pa[k]] * (i128)r[1 + pb[k]];
+                v = (float)((double)c / (nd * nd * unit * unit) * 12.0);
+            }
+            ft[5 + k] = v;
+        }
+        ft[11] = (float)eig[i].surface_variation * 3.0f;
+        ft[12] = (float)eig[i].planarity;
+        const float fill = is_leaf(n) ? (float)n->num_points * (1.0f / 50000.0f) : (float)n->num_voxels * (1.0f / 16384.0f);
+        ft[13] = fminf(fill, 4.0f);
+        float cvar = 0.0f;
+        if (cnt >= 2) {
+            const uint64_t* c = col + (size_t)i * 6;
+            for (int k = 0; k < 3; k++) {
+                const double m = (double)c[k] / nd;
+                cvar += (float)(((double)c[3 + k] / nd - m * m) / (255.0 * 255.0));
+            }
+        }
+        ft[14] = cvar * (4.0f / 3.0f);
+        const float age = current_batch > lt[i] ? (float)(current_batch - lt[i]) : 0.0f;
+        ft[15] = fminf(age / (float)(closure_margin ? closure_margin : 1u), 2.0f);
+    }
+    free(sums);
+    free(lt);
+    free(col);
+    free(eig);
+}
+
 static void box_extent(const or_frame* f, float cube, uint32_t level, uint32_t X, uint32_t Y, uint32_t Z,
                        float ext[4], int* any);
 

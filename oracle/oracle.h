@@ -186,6 +186,10 @@ typedef struct or_analysis_params {
  * (surface variation x coverage, 0 below min_points) per node, from
  * or_analyze_fp64's eigenvalues; the projected extents use the LOD cut's float
  * arithmetic (remolod_render.cu:40-70). */
+/* The learned scorer's 16 inputs per node as rb_analyze logs them (out16:
+ * num_nodes x 16 floats); surface variation and planarity from the FP64
+ * eigen-solve. */
+void or_features(const or_tree* t, uint32_t current_batch, uint32_t closure_margin, float* out16);
 void or_analysis_scores(const or_tree* t, const or_frame* f, const or_analysis_params* p,
                         const or_analysis_node* eig, float* coverage, uint32_t* flags, uint32_t* closed,
                         double* score);

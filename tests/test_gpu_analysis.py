@@ -160,3 +160,19 @@ def test_colour_filtering_matches_oracle_and_lifts_psnr(c1_cloud):
     r2 = ctx.refine_colors(len(queue))
     assert r2.voxels_filtered == r.voxels_filtered
     compare_voxels(ctx, tree, ctx.nodes())
+
+
+def test_logged_features_match_oracle(analysed):
+    """The training-data logger's 16 features per node (rb_read_features)
+    against the oracle's restatement: counts, level, means, second moments,
+    fill, colour variance and age from the same exact sums (float rounding
+    only); surface variation and planarity within the eigen-solve tolerance."""
+    ctx, tree, f, r = analysed
+    g = ctx.features()
+    o = tree.features(8, 8)  # the fixture analysed after 8 batches with closure margin 8
+    assert g.shape == o.shape
+    exact_cols = [0, 1, 2, 3, 4, 13, 14, 15]
+    assert np.allclose(g[:, exact_cols], o[:, exact_cols], rtol=1e-6, atol=1e-7)
+    assert np.allclose(g[:, 5:11], o[:, 5:11], rtol=1e-5, atol=1e-7)  # 128-bit -> double conversions
+    assert np.max(np.abs(g[:, 11] - o[:, 11])) <= 3 * SV_ATOL
+    assert np.max(np.abs(g[:, 12] - o[:, 12])) <= 1e-3

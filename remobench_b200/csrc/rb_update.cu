@@ -297,13 +297,17 @@ __global__ void __launch_bounds__(256) k_count_first(Dev d, const Point* __restr
 // same launch.
 //
 // prevStamp == 0: device-driven; the stamp of the last split's first round,
-// and no recount once the pass limit is reached.
+// and no counting (only moving) once the pass limit is reached.
 __device__ __forceinline__ void recountBody(const Dev& d, const Point* __restrict__ pts, uint32_t n,
                                             uint32_t prevStamp, uint32_t gated) {
     Counters* c = d.ctr;
     if (c->batchStop || (gated && c->loopMore == 0u)) return;
+    // Past the pass limit the loop counts no more (the nodes the last split
+    // made keep counter 0), but points still move to their leaves: insertion
+    // stores a point in the leaf the finished tree gives it.
+    bool counting = true;
     if (prevStamp == 0u) {
-        if (c->iter > d.maxExpandIters) return;
+        counting = c->iter <= d.maxExpandIters;
         prevStamp = c->lastStamp;
     }
     RB_BATCH_AT_CURSOR(d, pts, n);
@@ -335,7 +339,7 @@ __device__ __forceinline__ void recountBody(const Dev& d, const Point* __restric
                 }
                 if (batchPt) d.leafOf[i] = cur;
                 else d.spillLeaf[i - n] = cur;
-                if (cur >= lo && cur < hi)
+                if (counting && cur >= lo && cur < hi)
                     bin = cur * 8u + (lv < (uint32_t)kMaxDepth ? childIndex(x, y, z, lv) : 0u);
             }
         }

@@ -487,14 +487,24 @@ static void ensure_vox_cap(onode* n, uint32_t cap) {
     n->vox_cap = cap;
 }
 
-/* allocatePointChunks (remolod_octree.cu:742-792) */
-static void alloc_point_chunks(or_tree* t) {
+/* allocatePointChunks (remolod_octree.cu:742-792). The reference sizes a
+ * leaf's chunks by its counter, which equals its stored points plus the
+ * batch's arrivals whenever every leaf was counted in the batch it was made.
+ * A build whose expand loop stops at its pass limit leaves the last split's
+ * nodes uncounted (counter 0, later lagging their stored points), where the
+ * reference's rule would drop points (and its chunk walk has no defined
+ * result); here the need is the larger of the two, so every arriving point
+ * has a slot and the rule is the reference's wherever counters are whole.
+ * arrivals[i]: the points of this batch whose leaf is node i. */
+static void alloc_point_chunks(or_tree* t, const uint32_t* arrivals) {
     const uint32_t ppc = t->cfg.points_per_chunk;
     const uint64_t pool_before = t->st.chunk_pool_size;
     for (uint32_t i = 0; i < t->num_nodes; i++) {
         onode* n = &t->nodes[i];
-        if (!is_leaf(n) || !(n->num_points < n->counter)) continue;
-        uint32_t required = ceil_div(n->counter, ppc);
+        const uint32_t reach = n->num_points + arrivals[i];
+        const uint32_t need = n->counter > reach ? n->counter : reach;
+        if (!is_leaf(n) || !(n->num_points < need)) continue;
+        uint32_t required = ceil_div(need, ppc);
         uint32_t existing = ceil_div(n->num_points, ppc);
         if (required <= existing) continue;
         uint32_t extra = required - existing;
@@ -571,18 +581,23 @@ int or_add_batch(or_tree* t, const or_point* pts, uint32_t n) {
     vbacklog bl = {NULL, 0, 0};
     sample_all(t, pts, n, &bl);
 
-    alloc_point_chunks(t);
-    alloc_voxel_chunks(t);
-
-    /* insertPoints: leaves in parallel (the tree is fixed now), slots in order */
+    /* insertPoints' leaves: in parallel (the tree is fixed now) */
     const uint64_t total = (uint64_t)n + t->spill_n;
     uint32_t* leaves = (uint32_t*)malloc((size_t)(total ? total : 1) * sizeof(uint32_t));
-    if (!leaves) abort();
+    uint32_t* arrivals = (uint32_t*)calloc(t->num_nodes ? t->num_nodes : 1, sizeof(uint32_t));
+    if (!leaves || !arrivals) abort();
     const int nth = or_threads(t);
     const int64_t tot = (int64_t)total;
 #pragma omp parallel for num_threads(nth) schedule(static) if (nth > 1)
     for (int64_t i = 0; i < tot; i++)
         leaves[i] = leaf_of(t, i < (int64_t)n ? &pts[i] : &t->spill[i - (int64_t)n].p);
+    for (uint64_t i = 0; i < total; i++) arrivals[leaves[i]]++;
+
+    alloc_point_chunks(t, arrivals);
+    alloc_voxel_chunks(t);
+    free(arrivals);
+
+    /* insertPoints: slots in order */
     for (uint32_t i = 0; i < n; i++) insert_at(t, leaves[i], &pts[i], first_index + i);
     for (uint64_t i = 0; i < t->spill_n; i++) insert_at(t, leaves[n + i], &t->spill[i].p, t->spill[i].index);
     free(leaves);

@@ -582,6 +582,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.accumTo, N, "accumulate plan ranges");
     ALLOC(d.accumItem, (uint64_t)N + 1, "accumulate plan items");
     ALLOC(d.hist8, (uint64_t)N * 8, "child-octant counts");
+    ALLOC(d.arrive, N, "points reaching each leaf");
     ALLOC(d.deepCnt, (uint64_t)rb::kDeepRoots * rb::kDeepCells, "expand round bins");
     ALLOC(d.deepSlot, N, "expand round root slots");
     ALLOC(d.deepMeta, N, "expand round node codes");
@@ -626,6 +627,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     RB_CUDA(c, cudaMemsetAsync(d.hashSlots, 0xFF, (size_t)hashSize * 16, c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.ctr, 0, sizeof(Counters), c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.deepCnt, 0, (size_t)rb::kDeepRoots * rb::kDeepCells * 4, c->stream));
+    RB_CUDA(c, cudaMemsetAsync(d.arrive, 0, (size_t)N * 4, c->stream));
     RB_CUDA(c, cudaMemsetAsync(c->refine.refSlot, 0xFF, (size_t)N * 4, c->stream));
     RB_CUDA(c, cudaMemsetAsync(c->refine.hashKeys, 0xFF, ((size_t)c->refine.hashMask + 1) * 8, c->stream));
     RB_CUDA(c, cudaMallocHost(&c->hostRefine, sizeof(rb::RefineCounters)));

@@ -94,6 +94,11 @@ struct Counters {
     // grid barrier of the cooperative expand kernel (k_expand_rest), per batch
     uint32_t barArrive;
     uint32_t barRelease;
+    // set by the first batch whose expand loop stopped at its pass limit
+    // (until the next reset): its last split's nodes were not counted, so
+    // leaves' counters may lag their points, and point chunks are sized from
+    // the points that reach each leaf (Dev::arrive)
+    uint32_t arrivalMode;
 };
 
 enum StopReason : uint32_t { kStopMemory = 1u, kStopNoBatch = 2u, kStopTime = 3u };
@@ -230,6 +235,9 @@ struct Dev {
     // per node, its points per child octant, counted by the recount for the
     // nodes made by the last split: one level of lookahead for the next split
     uint32_t* hist8;         // [maxNodes * 8]
+    // per node, the batch's points whose leaf it is; counted by k_vox_sample
+    // and cleared by k_alloc_chunks, in arrival mode only (Counters::arrivalMode)
+    uint32_t* arrive;        // [maxNodes]
     // multi-level expand round: per root slot, the points below it counted at
     // every depth 1..kDeepLevels ([kDeepRoots][kDeepCells]); per root node its
     // slot; per node made by the round, (slot << 16) | its code below the root;

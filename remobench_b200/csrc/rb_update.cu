@@ -1453,6 +1453,7 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
     // the expand loop stopped at its pass limit: a point's recorded leaf may
     // have been split after its last count, so finish its descent
     const bool mayBeStale = c->iter > d.maxExpandIters;
+    const bool countArrivals = mayBeStale || c->arrivalMode != 0u;
     const bool lowest = d.voxelMode == 0u;
     const uint32_t lane = laneId();
     const uint32_t per = (((total + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
@@ -1481,13 +1482,24 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
                 const uint32_t x20 = quant20(p.x, d.boxMin[0], d.octreeSize),
                                y20 = quant20(p.y, d.boxMin[1], d.octreeSize),
                                z20 = quant20(p.z, d.boxMin[2], d.octreeSize);
+                const uint32_t from = leaf;
                 while (lv < (uint32_t)kMaxDepth) {
                     const int32_t nx = d.child[leaf * 8u + childIndex(x20, y20, z20, lv)];
                     if (nx < 0) break;
                     leaf = (uint32_t)nx;
                     lv += 1u;
                 }
+                // insertion stores the point in the leaf counted here
+                if (leaf != from) {
+                    if (i < n) d.leafOf[i] = leaf;
+                    else d.spillLeaf[i - n] = leaf;
+                }
             }
+        }
+        // arrival mode: the points reaching each leaf, for k_alloc_chunks
+        if (countArrivals) {
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, active ? leaf : kNone);
+            if (active && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&d.arrive[leaf], (uint32_t)__popc(peers));
         }
         // (1) which levels' cells were empty before this batch
         const uint2* row = d.anc + (size_t)leaf * kMaxDepth;
@@ -1770,9 +1782,20 @@ __global__ void __launch_bounds__(256) k_alloc_chunks(Dev d) {
     const uint32_t nn = c->numNodes;
     const uint32_t poolBefore = c->chunkPoolSize;
     const uint32_t ppc = d.ppc;
+    // A leaf's counter is its stored points plus this batch's arrivals while
+    // every leaf is counted in the batch it is made in (the reference's rule
+    // sizes by the counter). Once an expand loop stopped at its pass limit,
+    // the need is the larger of the counter and the points that reach it.
+    const bool arrivals = c->arrivalMode != 0u || c->iter > d.maxExpandIters;
     for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < nn;
          node += gridDim.x * blockDim.x) {
-        const uint32_t npts = d.numPoints[node], cnt = d.counter[node];
+        const uint32_t npts = d.numPoints[node];
+        uint32_t cnt = d.counter[node];
+        if (arrivals) {
+            const uint32_t reach = npts + d.arrive[node];
+            d.arrive[node] = 0;
+            if (reach > cnt) cnt = reach;
+        }
         if (npts < cnt && isLeaf(d, node)) {
             const uint32_t req = (cnt + ppc - 1u) / ppc;
             const uint32_t ex = (npts + ppc - 1u) / ppc;
@@ -1937,6 +1960,7 @@ __global__ void k_batch_end(Dev d, uint32_t n) {
     c->numPointsProcessed += n;
     c->spilledPointsTotal += c->numSpilled;
     c->expandIters += c->iter < d.maxExpandIters ? c->iter : d.maxExpandIters;
+    if (c->iter > d.maxExpandIters) c->arrivalMode = 1u;
 }
 
 // Stats sweep (remolod_octree.cu:1271-1310).

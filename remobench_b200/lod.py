@@ -69,9 +69,15 @@ class Context:
         self.box_max = None
 
     def close(self):
-        if getattr(self, "h", None):
-            capi.lib().rb_destroy(self.h)
-            self.h = None
+        h = getattr(self, "h", None)
+        if not h:
+            return
+        self.h = None
+        # at interpreter exit the module's globals may already be gone; the
+        # process ending releases the context then
+        lib = getattr(capi, "lib", None)
+        if callable(lib):
+            lib().rb_destroy(h)
 
     def __del__(self):
         self.close()

@@ -140,7 +140,9 @@ def test_colour_filtering_matches_oracle_and_lifts_psnr(c1_cloud):
     cfg, cloud, bmin, bmax = c1_cloud
     ctx, _ = build_gpu(cloud, bmin, bmax, cfg.batch_size, refine_voxel_capacity=400000)
     tree = build_oracle(cloud, bmin, bmax, cfg.batch_size)
-    f = make_frame(bmin, bmax, W, H, yaw=1.3, pitch=-0.5, radius_scale=0.5, budget=64.0)
+    # a cut coarse enough that voxels are drawn (at 64 px every node on this
+    # view opens down to its leaves and the frame equals the flat render)
+    f = make_frame(bmin, bmax, W, H, yaw=1.3, pitch=-0.5, radius_scale=0.5, budget=256.0)
     flat = Context(pipeline=capi.RB_PIPELINE_FLAT)
     flat.allocate(len(cloud), bmin, bmax)
     dev = torch.from_numpy(cloud.view(np.float32).reshape(-1, 4)).cuda()

@@ -9,7 +9,9 @@ representatives and of kernel_accum_verify's invariants:
   kernels on a B200);
 - the node-pool guard that refuses splits once the pool is full (:309-321);
 - the expand pass limit (:402-462), where a point's recorded leaf may be split
-  after its last count and the later phases finish its descent;
+  after its last count and the later phases finish its descent, and point
+  chunks are sized from the points that reach each leaf (the last split's
+  nodes were never counted), so nothing is dropped;
 - first-come voxel representatives are members of their cell, on every node;
 - kernel_accum_verify's globals (remolod_accum.cu:214-233).
 """
@@ -105,15 +107,21 @@ def test_node_pool_guard_refuses_splits(c1_cloud, max_nodes):
 def test_expand_pass_limit(c1_cloud, iters, graphs):
     """max_expand_iters below what a batch needs: the loop stops with nodes
     still over the limit, points whose leaf split after their last count go on
-    descending in voxel sampling and insertion, and every structure equals the
-    oracle's with the same limit -- on the device graph and the host loop."""
+    descending in voxel sampling and insertion, chunks cover every point that
+    reaches a leaf (counters of the uncounted nodes stay 0 or lag), and every
+    structure equals the oracle's with the same limit -- on the device graph
+    and the host loop."""
     cfg, cloud, bmin, bmax = c1_cloud
     ctx, _ = build_gpu(cloud, bmin, bmax, cfg.batch_size, max_expand_iters=iters, use_graphs=graphs)
     tree = build_oracle(cloud, bmin, bmax, cfg.batch_size, max_expand_iters=iters)
     tree.accumulate(8)
     nodes = full_compare(ctx, tree)
-    # the limit bit: some leaf ends a batch above the split threshold
+    # the limit bit: some leaf ends a batch above the split threshold, and
+    # some leaf holds more points than its counter says
     assert int(nodes["num_points"].max()) > 50000
+    assert np.any(nodes["num_points"] > nodes["counter"])
+    s = ctx.stats()
+    assert s.dropped_points == 0 and s.num_points == len(cloud)
 
 
 def test_first_come_representatives_are_members_of_their_cell(c1_cloud):

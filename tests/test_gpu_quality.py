@@ -25,6 +25,9 @@ def test_lod_converges_to_flat(c1_cloud):
     view = dict(yaw=0.9, pitch=-0.45, radius_scale=0.5)
     tiny = quality.compare(ctx, flat, dev, make_frame(bmin, bmax, W, H, budget=1e-6, **view))
     assert tiny["psnr"] == float("inf") and tiny["coverage"] == 1.0 and tiny["depth_rel_rmse"] == 0.0
+    # budgets up to a few pixels still open every node on this view (the
+    # render is exact); coarser cuts draw voxels and drift from the flat image
     psnrs = [quality.compare(ctx, flat, dev, make_frame(bmin, bmax, W, H, budget=b, **view))["psnr"]
              for b in (8.0, 64.0, 512.0)]
-    assert all(np.isfinite(psnrs)) and psnrs[0] >= psnrs[-1]
+    assert all(a >= b for a, b in zip(psnrs, psnrs[1:])), psnrs
+    assert np.isfinite(psnrs[-1]) and psnrs[-1] < 40.0, psnrs

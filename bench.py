@@ -474,6 +474,12 @@ def main():
                          f"{threads} threads",
                "identity": sample_identity(pts, args.cpu_sample_batches)}
 
+    # the reference's own kernels over the same cloud on this GPU, beside the
+    # line's value (not part of it)
+    ref_kernels = None
+    if rank == 0 and world == 1 and not args.no_reference_kernels:
+        ref_kernels = reference_kernels_b200(pts, bmin, bmax)
+
     if rank == 0:
         p50 = float(np.percentile(frame_ms, 50)) if frame_ms else None
         p99 = float(np.percentile(frame_ms, 99)) if frame_ms else None
@@ -498,6 +504,7 @@ def main():
             "e2e": e2e,
             "clocks": clk,
             "generate_s": round(gen_s, 1),
+            "reference_kernels_b200": ref_kernels,
             "kernels": {k: {"launches": v["launches"] // 1, "ms": round(v["ms"], 3)} for k, v in
                         sorted(upd.items(), key=lambda kv: -kv[1]["ms"])},
         }

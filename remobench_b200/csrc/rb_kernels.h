@@ -49,7 +49,9 @@ void launchExpandCond(const Dev& d, cudaStream_t s);
 void launchSpillCopy(const Dev& d, int grid, cudaStream_t s);
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchVoxCommit(const Dev& d, int grid, cudaStream_t s);
-void launchAllocChunks(const Dev& d, int grid, cudaStream_t s);
+void launchFinishLeaves(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
+void launchAllocPoints(const Dev& d, int grid, cudaStream_t s);
+void launchAllocVoxels(const Dev& d, int grid, cudaStream_t s);
 void launchInsert(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchVoxStore(const Dev& d, int grid, cudaStream_t s);
 void launchBatchEnd(const Dev& d, uint32_t n, cudaStream_t s);

@@ -235,8 +235,9 @@ struct Dev {
     // per node, its points per child octant, counted by the recount for the
     // nodes made by the last split: one level of lookahead for the next split
     uint32_t* hist8;         // [maxNodes * 8]
-    // per node, the batch's points whose leaf it is; counted by k_vox_sample
-    // and cleared by k_alloc_chunks, in arrival mode only (Counters::arrivalMode)
+    // per node, the batch's points whose leaf it is; counted after the expand
+    // loop (finishLeavesBody) and cleared by k_alloc_points, in arrival mode
+    // only (Counters::arrivalMode)
     uint32_t* arrive;        // [maxNodes]
     // multi-level expand round: per root slot, the points below it counted at
     // every depth 1..kDeepLevels ([kDeepRoots][kDeepCells]); per root node its

@@ -958,12 +958,63 @@ __device__ __forceinline__ void bookSplit(const Dev& d, Counters* c, uint32_t no
     }
 }
 
+// Root k of the round: its split bookkeeping and its record for k_deep_bin
+// (spill slots from prePts, copy items from preCh).
+__device__ __forceinline__ void deepBookRoot(const Dev& d, Counters* c, uint32_t k, uint32_t node, uint32_t np,
+                                             uint32_t owned, uint32_t spillBase, uint32_t chunkBase, uint32_t stamp) {
+    bookSplit(d, c, node, stamp);
+    SplitRec r;
+    r.node = node;
+    r.numPoints = np;
+    r.tableOff = d.ptTableOff[node];
+    r.spillBase = spillBase;
+    r.chunkBase = chunkBase;
+    r.numChunks = owned;
+    r.grid = d.grid[node];
+    // the node's chunks go back to the queue (remolod_octree.cu:349-360)
+    r.queueBase = owned ? atomicSub(&c->numAllocatedChunks, owned) - owned : kNone;
+    d.splitRecs[k] = r;
+    d.numPoints[node] = 0;
+    d.numPointChunks[node] = 0;
+    d.ptTableOff[node] = kNone;
+    d.ptTableCap[node] = 0;
+    d.deepSlot[node] = k;
+}
+
+// The round's counters, by one thread.
+__device__ __forceinline__ void deepBookCounters(const Dev& d, Counters* c, uint32_t ns, uint32_t acc,
+                                                 uint32_t spilledBefore, uint32_t totPts, uint32_t totCh,
+                                                 uint32_t stamp, uint32_t levels, uint32_t n0) {
+    if (acc < ns) c->nodePoolOverflow = 1;
+    uint32_t total = spilledBefore + totPts;
+    if (total > d.spillCap) {
+        atomicOr(&c->overflowFlags, (uint32_t)kOvfSpilled);
+        total = d.spillCap;
+    }
+    c->numSpilled = total;
+    c->numSplit = acc;
+    c->spillChunkTotal = totCh;
+    c->nodesSplit += acc;
+    c->numSpill = 0;
+    c->lastStamp = stamp;
+    c->histValid = 0;
+    c->countLo = 0;
+    c->countHi = 0;
+    c->deepRoots = acc;
+    c->deepLevels = levels;
+    c->deepBase = n0;
+    c->deepStamp = stamp;
+    c->deepActive = 1;
+}
+
 // Iteration 1's splits (doSplitting for the first count's spilling nodes, in
 // increasing id): their bookkeeping, where their stored points go in the
 // spill list, their chunks' queue positions. The children are made by
-// k_deep_split with the later generations. One block of 1024 threads. Leaves
-// the round off (the per-iteration passes take the batch) when no node can
-// be split, more than kDeepRoots spill, or a root lies too deep to bin below.
+// k_deep_split with the later generations. One block of 1024 threads; up to
+// 32 roots (most batches) are sorted, scanned and booked by one warp with no
+// block barrier. Leaves the round off (the per-iteration passes take the
+// batch) when no node can be split, more than kDeepRoots spill, or a root
+// lies too deep to bin below.
 __global__ void __launch_bounds__(1024) k_deep_book(Dev d) {
     __shared__ uint32_t s_sort[kDeepRoots];
     __shared__ uint32_t s_warp[32];
@@ -977,6 +1028,37 @@ __global__ void __launch_bounds__(1024) k_deep_book(Dev d) {
     const uint32_t room = d.maxNodes > n0 ? (d.maxNodes - n0) / 8u : 0u;
     const uint32_t acc = ns < room ? ns : room;
     if (acc == 0u) return;
+    const uint32_t stamp = (c->batchletIndex << 5) | c->iter;
+    const uint32_t spilledBefore = c->numSpilled;
+    if (ns <= 32u) {
+        if (threadIdx.x >= 32u) return;
+        const uint32_t lane = threadIdx.x;
+        const uint32_t node = warpSortAscending(lane < ns ? d.spillNodes[lane] : kNone);
+        const uint32_t maxLevel = __reduce_max_sync(0xFFFFFFFFu, lane < acc ? d.level[node] : 0u);
+        if (maxLevel >= (uint32_t)kMaxDepth) return;
+        const uint32_t depthRoom = (uint32_t)kMaxDepth - maxLevel;
+        const uint32_t levels = depthRoom < kDeepLevels ? depthRoom : kDeepLevels;
+        uint32_t np = 0, owned = 0;
+        if (lane < acc) {
+            owned = d.numPointChunks[node];
+            const uint32_t cap = owned * d.ppc;
+            np = d.numPoints[node] < cap ? d.numPoints[node] : cap;
+        }
+        uint32_t xp = np, xc = owned;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t yp = __shfl_up_sync(0xFFFFFFFFu, xp, o);
+            const uint32_t yc = __shfl_up_sync(0xFFFFFFFFu, xc, o);
+            if (lane >= (uint32_t)o) {
+                xp += yp;
+                xc += yc;
+            }
+        }
+        const uint32_t totPts = __shfl_sync(0xFFFFFFFFu, xp, 31), totCh = __shfl_sync(0xFFFFFFFFu, xc, 31);
+        if (lane < acc) deepBookRoot(d, c, lane, node, np, owned, spilledBefore + xp - np, xc - owned, stamp);
+        if (lane == 0u) deepBookCounters(d, c, ns, acc, spilledBefore, totPts, totCh, stamp, levels, n0);
+        return;
+    }
     for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) s_sort[i] = d.spillNodes[i];
     if (threadIdx.x == 0) s_maxLevel = 0;
     __syncthreads();
@@ -987,9 +1069,6 @@ __global__ void __launch_bounds__(1024) k_deep_book(Dev d) {
     if (maxLevel >= (uint32_t)kMaxDepth) return;
     const uint32_t depthRoom = (uint32_t)kMaxDepth - maxLevel;
     const uint32_t levels = depthRoom < kDeepLevels ? depthRoom : kDeepLevels;
-    const uint32_t it0 = c->iter;
-    const uint32_t stamp = (c->batchletIndex << 5) | it0;
-    const uint32_t spilledBefore = c->numSpilled;
     // acc <= kDeepRoots < blockDim.x: one scan covers every root
     const uint32_t k = threadIdx.x;
     uint32_t node = 0, np = 0, owned = 0;
@@ -1002,54 +1081,39 @@ __global__ void __launch_bounds__(1024) k_deep_book(Dev d) {
     uint32_t totPts, totCh;
     const uint32_t prePts = blockExclusiveScan(np, &totPts, s_warp);
     const uint32_t preCh = blockExclusiveScan(owned, &totCh, s_warp);
-    if (k < acc) {
-        bookSplit(d, c, node, stamp);
-        SplitRec r;
-        r.node = node;
-        r.numPoints = np;
-        r.tableOff = d.ptTableOff[node];
-        r.spillBase = spilledBefore + prePts;
-        r.chunkBase = preCh;
-        r.numChunks = owned;
-        r.grid = d.grid[node];
-        // the node's chunks go back to the queue (remolod_octree.cu:349-360)
-        r.queueBase = owned ? atomicSub(&c->numAllocatedChunks, owned) - owned : kNone;
-        d.splitRecs[k] = r;
-        d.numPoints[node] = 0;
-        d.numPointChunks[node] = 0;
-        d.ptTableOff[node] = kNone;
-        d.ptTableCap[node] = 0;
-        d.deepSlot[node] = k;
+    if (k < acc) deepBookRoot(d, c, k, node, np, owned, spilledBefore + prePts, preCh, stamp);
+    if (threadIdx.x == 0) deepBookCounters(d, c, ns, acc, spilledBefore, totPts, totCh, stamp, levels, n0);
+}
+
+// A block's bin counts, merged in shared memory before they reach the global
+// bins: the coarse cubes (8 per root at depth 1) are shared by most of a
+// batch's points, and one global atomic per warp on them serialises in one L2
+// slice. Keys are bin indices (slot * kDeepCells + cube), below 2^22.
+constexpr uint32_t kDeepBlockBins = 1024;
+struct DeepBlockBins {
+    uint32_t key[kDeepBlockBins];
+    uint32_t cnt[kDeepBlockBins];
+};
+
+__device__ __forceinline__ void deepBinsInit(DeepBlockBins& b) {
+    for (uint32_t t = threadIdx.x; t < kDeepBlockBins; t += blockDim.x) {
+        b.key[t] = kNone;
+        b.cnt[t] = 0;
     }
-    if (threadIdx.x == 0) {
-        if (acc < ns) c->nodePoolOverflow = 1;
-        uint32_t total = spilledBefore + totPts;
-        if (total > d.spillCap) {
-            atomicOr(&c->overflowFlags, (uint32_t)kOvfSpilled);
-            total = d.spillCap;
-        }
-        c->numSpilled = total;
-        c->numSplit = acc;
-        c->spillChunkTotal = totCh;
-        c->nodesSplit += acc;
-        c->numSpill = 0;
-        c->lastStamp = stamp;
-        c->histValid = 0;
-        c->countLo = 0;
-        c->countHi = 0;
-        c->deepRoots = acc;
-        c->deepLevels = levels;
-        c->deepBase = n0;
-        c->deepStamp = stamp;
-        c->deepActive = 1;
-    }
+}
+
+// After a barrier: the block's counts into the global bins.
+__device__ __forceinline__ void deepBinsFlush(const Dev& d, DeepBlockBins& b) {
+    for (uint32_t t = threadIdx.x; t < kDeepBlockBins; t += blockDim.x)
+        if (b.key[t] != kNone && b.cnt[t] != 0u) atomicAdd(&d.deepCnt[b.key[t]], b.cnt[t]);
 }
 
 // One point below root slot `slot` (at level lv) into its cubes at depths
 // 1..levels. Every lane of the warp calls it; lanes with no point pass
-// active = false. Equal cubes in a warp add once.
-__device__ __forceinline__ void deepBin(const Dev& d, bool active, uint32_t slot, uint32_t lv, const Point& p,
-                                        uint32_t levels) {
+// active = false. Equal cubes in a warp add once, into the block's table
+// (or straight into the global bin when its probe run is full).
+__device__ __forceinline__ void deepBin(const Dev& d, DeepBlockBins& bins, bool active, uint32_t slot, uint32_t lv,
+                                        const Point& p, uint32_t levels) {
     uint32_t x = 0, y = 0, z = 0;
     if (active) {
         x = quant20(p.x, d.boxMin[0], d.octreeSize);
@@ -1063,18 +1127,36 @@ __device__ __forceinline__ void deepBin(const Dev& d, bool active, uint32_t slot
         code = (code << 3) | (active ? childIndex(x, y, z, lv + j - 1u) : 0u);
         const uint32_t key = active ? slot * kDeepCells + deepOffset(j) + code : kNone;
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
-        if (active && (int)laneId() == __ffs(peers) - 1) atomicAdd(&d.deepCnt[key], (uint32_t)__popc(peers));
+        if (active && (int)laneId() == __ffs(peers) - 1) {
+            const uint32_t g = (uint32_t)__popc(peers);
+            uint32_t h = (key * 0x9E3779B1u) >> 22;
+            bool done = false;
+            for (uint32_t probe = 0; probe < 8u; probe++) {
+                const uint32_t cur = atomicCAS(&bins.key[h], kNone, key);
+                if (cur == kNone || cur == key) {
+                    atomicAdd(&bins.cnt[h], g);
+                    done = true;
+                    break;
+                }
+                h = (h + 1u) & (kDeepBlockBins - 1u);
+            }
+            if (!done) atomicAdd(&d.deepCnt[key], g);
+        }
     }
 }
 
 // The roots' stored points move to the spill list (remolod_octree.cu:250-285)
 // and their chunks return to the queue (:349-360), one work item per owned
-// chunk; then every batch point whose leaf is a root. Each is binned below its
-// root.
+// chunk; then every batch point whose leaf is a root, each block a contiguous
+// run of the batch (neighbouring points share cubes). Each is binned below
+// its root.
 __global__ void __launch_bounds__(256) k_deep_bin(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    __shared__ DeepBlockBins s_bins;
     const Counters* c = d.ctr;
     if (c->batchStop || !c->deepActive) return;
     RB_BATCH_AT_CURSOR(d, pts, n);
+    deepBinsInit(s_bins);
+    __syncthreads();
     const uint32_t levels = c->deepLevels, stamp = c->deepStamp;
     const uint32_t nsplit = c->numSplit, nchunk = c->spillChunkTotal;
     for (uint32_t w = blockIdx.x; w < nchunk; w += gridDim.x) {
@@ -1103,27 +1185,32 @@ __global__ void __launch_bounds__(256) k_deep_bin(Dev d, const Point* __restrict
                 d.spillIdx[slot] = chunkIndices(d, phys)[s - first];
                 d.spillLeaf[slot] = r.node;
             }
-            deepBin(d, active, lo, lv, q, levels);
+            deepBin(d, s_bins, active, lo, lv, q, levels);
         }
     }
-    for (uint32_t b = blockIdx.x * blockDim.x; b < n; b += gridDim.x * blockDim.x) {
-        const uint32_t i = b + threadIdx.x;
+    const uint32_t per = (((n + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
+    const uint32_t begin = min(n, blockIdx.x * per), end = min(n, begin + per);
+    for (uint32_t base = begin; base < end; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
         uint32_t leaf = 0;
         bool active = false;
-        if (i < n) {
+        Point p = {0.f, 0.f, 0.f, 0u};
+        if (i < end) {
+            // the point with its leaf: one round trip instead of two
+            p = loadPoint(pts + i);
             leaf = d.leafOf[i];
             active = d.splitIter[leaf] == stamp;
         }
         if (!__any_sync(0xFFFFFFFFu, active)) continue;
-        Point p = {0.f, 0.f, 0.f, 0u};
         uint32_t slot = 0, lv = 0;
         if (active) {
-            p = loadPoint(pts + i);
             slot = d.deepSlot[leaf];
             lv = d.level[leaf];
         }
-        deepBin(d, active, slot, lv, p, levels);
+        deepBin(d, s_bins, active, slot, lv, p, levels);
     }
+    __syncthreads();
+    deepBinsFlush(d, s_bins);
 }
 
 // Iterations 2 .. 1 + kDeepLevels from the binned counts: generation g (the
@@ -1136,7 +1223,6 @@ __global__ void __launch_bounds__(256) k_deep_bin(Dev d, const Point* __restrict
 // 1024 threads.
 __global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
     __shared__ uint32_t s_warp[32];
-    __shared__ uint32_t s_acc, s_cont;
     Counters* c = d.ctr;
     if (c->batchStop || !c->deepActive) return;
     const uint32_t roots = c->deepRoots, levels = c->deepLevels, base = c->deepBase, it0 = c->iter;
@@ -1146,6 +1232,7 @@ __global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
         makeChild(d, base + t, d.splitRecs[t >> 3].node, t & 7u);
         d.deepMeta[t] = ((t >> 3) << 16) | (t & 7u);
     }
+    __syncthreads();
     uint32_t lo = base, hi = base + 8u * roots;
     uint32_t splits = 0, itEnd = 0, cont = 0;
     for (uint32_t g = 1;; g++) {
@@ -1155,11 +1242,8 @@ __global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
             break;
         }
         const uint32_t room = d.maxNodes > hi ? (d.maxNodes - hi) / 8u : 0u;
-        if (threadIdx.x == 0) {
-            s_acc = 0;
-            s_cont = 0;
-        }
-        __syncthreads();
+        // running totals, the same in every thread (the scan returns them to all)
+        uint32_t want = 0, contRun = 0;
         for (uint32_t t0 = lo; t0 < hi; t0 += blockDim.x) {
             const uint32_t node = t0 + threadIdx.x;
             uint32_t cnt = 0;
@@ -1171,34 +1255,31 @@ __global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
             const bool over = node < hi && cnt > d.maxPointsPerNode;
             const uint32_t wantSplit = (over && g < levels) ? 1u : 0u;
             const uint32_t wantCont = (over && g == levels) ? 1u : 0u;
-            uint32_t totS, totC;
-            const uint32_t preS = blockExclusiveScan(wantSplit, &totS, s_warp);
-            const uint32_t preC = blockExclusiveScan(wantCont, &totC, s_warp);
-            const uint32_t j = s_acc + preS;
+            // one scan for both lists: splits in the low half, continuations
+            // in the high half (at most blockDim.x of each per step)
+            uint32_t tot;
+            const uint32_t pre = blockExclusiveScan(wantSplit | (wantCont << 16), &tot, s_warp);
+            const uint32_t j = want + (pre & 0xFFFFu);
             if (wantSplit && j < room) {
                 bookSplit(d, c, node, batchTag | it);
                 d.deepPar[j] = node;
             }
-            const uint32_t jc = s_cont + preC;
+            const uint32_t jc = contRun + (pre >> 16);
             if (wantCont && jc < d.spillingCap) d.spillNodes[jc] = node;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                s_acc += totS;
-                s_cont += totC;
-            }
-            __syncthreads();
+            want += tot & 0xFFFFu;
+            contRun += tot >> 16;
         }
-        const uint32_t want = s_acc;
         const uint32_t nacc = want < room ? want : room;
         if (threadIdx.x == 0 && nacc < want) c->nodePoolOverflow = 1;
         if (nacc == 0u) {
-            cont = s_cont;
+            cont = contRun;
             // continuation: the per-iteration passes split them in this
             // iteration; every spiller refused: one more, empty, count
             itEnd = cont > 0u ? it : (want > 0u ? it + 1u : it);
             break;
         }
         splits += nacc;
+        __syncthreads();  // the split list (deepPar) and the parents' grids are written
         // the children of this iteration's splits, ids [hi, hi + 8 nacc)
         for (uint32_t t = threadIdx.x; t < 8u * nacc; t += blockDim.x) {
             const uint32_t parent = d.deepPar[t >> 3];
@@ -1277,6 +1358,58 @@ __device__ void zeroGridsBody(const Dev& d) {
 
 __global__ void __launch_bounds__(256) k_zero_grids(Dev d) { zeroGridsBody(d); }
 
+// After the expand loop, before voxel sampling and insertion. Once the loop
+// stopped at its pass limit, a point's recorded leaf may have been split
+// after its last count: its descent is finished here, so both sampling and
+// insertion read the leaf the finished tree gives it. In arrival mode
+// (Counters::arrivalMode, or this batch stopped at the limit) the points
+// reaching each leaf are counted for the point-chunk allocation. Otherwise
+// nothing to do: every recorded leaf is final and counters are whole.
+__device__ void finishLeavesBody(const Dev& d, const Point* __restrict__ pts, uint32_t n) {
+    const Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const bool stale = c->iter > d.maxExpandIters;
+    if (!stale && c->arrivalMode == 0u) return;
+    RB_BATCH_AT_CURSOR(d, pts, n);
+    const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
+    const uint32_t total = n + ns;
+    const uint32_t lane = laneId();
+    // the same number of steps in every lane of a warp
+    for (uint32_t b = blockIdx.x * blockDim.x; b < total; b += gridDim.x * blockDim.x) {
+        const uint32_t i = b + threadIdx.x;
+        const bool active = i < total;
+        uint32_t leaf = kNone;
+        if (active) {
+            const bool batchPt = i < n;
+            leaf = batchPt ? d.leafOf[i] : d.spillLeaf[i - n];
+            if (stale) {
+                const Point p = batchPt ? loadPoint(pts + i) : d.spillPts[i - n];
+                const uint32_t x = quant20(p.x, d.boxMin[0], d.octreeSize),
+                               y = quant20(p.y, d.boxMin[1], d.octreeSize),
+                               z = quant20(p.z, d.boxMin[2], d.octreeSize);
+                const uint32_t from = leaf;
+                uint32_t lv = d.level[leaf];
+                while (lv < (uint32_t)kMaxDepth) {
+                    const int32_t nx = d.child[leaf * 8u + childIndex(x, y, z, lv)];
+                    if (nx < 0) break;
+                    leaf = (uint32_t)nx;
+                    lv += 1u;
+                }
+                if (leaf != from) {
+                    if (batchPt) d.leafOf[i] = leaf;
+                    else d.spillLeaf[i - n] = leaf;
+                }
+            }
+        }
+        const unsigned peers = __match_any_sync(0xFFFFFFFFu, leaf);
+        if (active && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&d.arrive[leaf], (uint32_t)__popc(peers));
+    }
+}
+
+__global__ void __launch_bounds__(256) k_finish_leaves(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    finishLeavesBody(d, pts, n);
+}
+
 // Grid-wide barrier of a cooperative launch. Every block is resident, so the
 // wait ends once each block arrives; the polls are still bounded (about a
 // second), after which the block records kOvfSync, the others stop waiting
@@ -1340,6 +1473,7 @@ __global__ void __launch_bounds__(1024, 1) k_expand_rest(Dev d) {
         }
     }
     zeroGridsBody(d);
+    finishLeavesBody(d, nullptr, 0u);
 }
 
 __device__ __forceinline__ uint32_t hashSlot(unsigned long long key, uint32_t mask) {
@@ -1450,10 +1584,6 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
     const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
-    // the expand loop stopped at its pass limit: a point's recorded leaf may
-    // have been split after its last count, so finish its descent
-    const bool mayBeStale = c->iter > d.maxExpandIters;
-    const bool countArrivals = mayBeStale || c->arrivalMode != 0u;
     const bool lowest = d.voxelMode == 0u;
     const uint32_t lane = laneId();
     const uint32_t per = (((total + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
@@ -1478,28 +1608,6 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
             y28 = quant28(p.y, d.boxMin[1], d.octreeSize);
             z28 = quant28(p.z, d.boxMin[2], d.octreeSize);
             lv = d.level[leaf];
-            if (mayBeStale) {
-                const uint32_t x20 = quant20(p.x, d.boxMin[0], d.octreeSize),
-                               y20 = quant20(p.y, d.boxMin[1], d.octreeSize),
-                               z20 = quant20(p.z, d.boxMin[2], d.octreeSize);
-                const uint32_t from = leaf;
-                while (lv < (uint32_t)kMaxDepth) {
-                    const int32_t nx = d.child[leaf * 8u + childIndex(x20, y20, z20, lv)];
-                    if (nx < 0) break;
-                    leaf = (uint32_t)nx;
-                    lv += 1u;
-                }
-                // insertion stores the point in the leaf counted here
-                if (leaf != from) {
-                    if (i < n) d.leafOf[i] = leaf;
-                    else d.spillLeaf[i - n] = leaf;
-                }
-            }
-        }
-        // arrival mode: the points reaching each leaf, for k_alloc_chunks
-        if (countArrivals) {
-            const unsigned peers = __match_any_sync(0xFFFFFFFFu, active ? leaf : kNone);
-            if (active && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&d.arrive[leaf], (uint32_t)__popc(peers));
         }
         // (1) which levels' cells were empty before this batch
         const uint2* row = d.anc + (size_t)leaf * kMaxDepth;
@@ -1772,11 +1880,13 @@ __device__ __forceinline__ void markDirty(const Dev& d, uint32_t node) {
     else atomicOr(&c->overflowFlags, (uint32_t)kOvfDirty);
 }
 
-// allocatePointChunks (remolod_octree.cu:742-792) and allocateVoxelChunks
-// (:885-916), one thread per node. Chunk ids come from the recycled queue
-// first, then from the pool; the reference store's offset advances by one
-// chunk for every pool chunk, so memCapacityReached falls where it would.
-__global__ void __launch_bounds__(256) k_alloc_chunks(Dev d) {
+// allocatePointChunks (remolod_octree.cu:742-792), one thread per node. Chunk
+// ids come from the recycled queue first, then from the pool; the reference
+// store's offset advances by one chunk for every pool chunk, so
+// memCapacityReached falls where it would. It runs beside the voxel path
+// (k_vox_sample .. k_vox_store): the two share only the arena and table-pool
+// bump counters and the store offset, all advanced by atomics.
+__global__ void __launch_bounds__(256) k_alloc_points(Dev d) {
     Counters* c = d.ctr;
     if (c->batchStop) return;
     const uint32_t nn = c->numNodes;
@@ -1828,6 +1938,18 @@ __global__ void __launch_bounds__(256) k_alloc_chunks(Dev d) {
             }
             markDirty(d, node);
         }
+    }
+}
+
+// allocateVoxelChunks (:885-916), one thread per node, after k_vox_commit
+// has counted the batch's new voxels.
+__global__ void __launch_bounds__(256) k_alloc_voxels(Dev d) {
+    Counters* c = d.ctr;
+    if (c->batchStop) return;
+    const uint32_t nn = c->numNodes;
+    const uint32_t ppc = d.ppc;
+    for (uint32_t node = blockIdx.x * blockDim.x + threadIdx.x; node < nn;
+         node += gridDim.x * blockDim.x) {
         const uint32_t nv = d.numVoxels[node];
         const uint32_t reqv = (nv + ppc - 1u) / ppc;
         const uint32_t havev = d.numVoxelChunks[node];
@@ -2076,7 +2198,11 @@ void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaS
     k_vox_sample<<<grid, 256, 0, s>>>(d, pts, n);
 }
 void launchVoxCommit(const Dev& d, int grid, cudaStream_t s) { k_vox_commit<<<grid, 256, 0, s>>>(d); }
-void launchAllocChunks(const Dev& d, int grid, cudaStream_t s) { k_alloc_chunks<<<grid, 256, 0, s>>>(d); }
+void launchFinishLeaves(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
+    k_finish_leaves<<<grid, 256, 0, s>>>(d, pts, n);
+}
+void launchAllocPoints(const Dev& d, int grid, cudaStream_t s) { k_alloc_points<<<grid, 256, 0, s>>>(d); }
+void launchAllocVoxels(const Dev& d, int grid, cudaStream_t s) { k_alloc_voxels<<<grid, 256, 0, s>>>(d); }
 void launchInsert(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_insert<<<grid, 256, 0, s>>>(d, pts, n);
 }
@@ -2087,17 +2213,24 @@ void launchResetRoot(const Dev& d, int grid, cudaStream_t s) { k_reset_root<<<gr
 
 // One batch as a CUDA graph: the phase kernels of runBatch, every kernel
 // reading its batch from the device cursor, the expand round's leftovers in
-// the cooperative k_expand_rest. One graph launch builds the batch at
-// batchletIndex with no host round trip and no conditional node; a stopped
-// batch (memory, no batch uploaded, time budget) runs through as no-ops.
+// the cooperative k_expand_rest. After it the graph forks: the voxel path
+// (k_vox_sample, k_vox_commit, k_alloc_voxels, k_vox_store) and the point path
+// (k_alloc_points, k_insert) read the finished tree and write disjoint node
+// fields and chunks, so the point path runs in the voxel path's shadow; they
+// join before k_batch_end. One graph launch builds the batch at batchletIndex
+// with no host round trip and no conditional node; a stopped batch (memory,
+// no batch uploaded, time budget) runs through as no-ops.
 cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int restGrid, cudaGraphExec_t* out) {
     *out = nullptr;
-    cudaStream_t cs = nullptr;
+    cudaStream_t cs = nullptr, cs2 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return e;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
     bool capturing = false;
-    do {
+    while (e == cudaSuccess) {
         if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) break;
         capturing = true;
         k_batch_begin<<<1, 1, 0, cs>>>(d, 1u);
@@ -2107,24 +2240,33 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int re
         k_deep_split<<<1, 1024, 0, cs>>>(d);
         k_deep_move<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         if ((e = launchExpandRest(d, restGrid, cs)) != cudaSuccess) break;
+        if ((e = cudaEventRecord(fork, cs)) != cudaSuccess) break;
+        if ((e = cudaStreamWaitEvent(cs2, fork, 0)) != cudaSuccess) break;
+        k_alloc_points<<<fixedGrid, 256, 0, cs2>>>(d);
+        k_insert<<<pointGrid, 256, 0, cs2>>>(d, nullptr, 0u);
+        if ((e = cudaEventRecord(join, cs2)) != cudaSuccess) break;
         k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
         k_vox_commit<<<fixedGrid, 256, 0, cs>>>(d);
-        k_alloc_chunks<<<fixedGrid, 256, 0, cs>>>(d);
-        k_insert<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        k_alloc_voxels<<<fixedGrid, 256, 0, cs>>>(d);
         k_vox_store<<<fixedGrid, 256, 0, cs>>>(d);
+        if ((e = cudaStreamWaitEvent(cs, join, 0)) != cudaSuccess) break;
         k_batch_end<<<1, 1, 0, cs>>>(d, kNone);
         if ((e = cudaGetLastError()) != cudaSuccess) break;
         capturing = false;
         if ((e = cudaStreamEndCapture(cs, &graph)) != cudaSuccess) break;
         e = cudaGraphInstantiate(out, graph, 0ull);
-    } while (false);
+        break;
+    }
     if (capturing) {
         cudaGraph_t dropped = nullptr;
         cudaStreamEndCapture(cs, &dropped);
         if (dropped) cudaGraphDestroy(dropped);
     }
     if (graph) cudaGraphDestroy(graph);
-    cudaStreamDestroy(cs);
+    if (join) cudaEventDestroy(join);
+    if (fork) cudaEventDestroy(fork);
+    if (cs2) cudaStreamDestroy(cs2);
+    if (cs) cudaStreamDestroy(cs);
     if (e != cudaSuccess) {
         cudaGetLastError();
         *out = nullptr;

@@ -73,11 +73,6 @@ __device__ __forceinline__ bool leafRow(const Dev& d, uint32_t node) {
 }
 
 constexpr int kAccumThreads = 256;
-constexpr int kAccumWarps = kAccumThreads / 32;
-constexpr int kNumSums = 3 + 12 + 3 + 3;  // s1, s2 (lo, hi), c1, c2
-// Points per work item: a leaf's new range is split over several blocks, so
-// a fold over a few hundred big leaves still fills the GPU.
-constexpr uint32_t kAccumChunk = 4096;
 
 // 128-bit atomic add on a (lo, hi) pair: the add that wraps lo carries into hi.
 __device__ __forceinline__ void atomicAdd128(unsigned long long* lo, unsigned long long* hi,
@@ -87,25 +82,31 @@ __device__ __forceinline__ void atomicAdd128(unsigned long long* lo, unsigned lo
     if (vhi + carry) atomicAdd(hi, vhi + carry);
 }
 
-// The fold's plan (one block): the nodes to visit (the dirty list, or every
-// node), each leaf's new range [count, min(numPoints, capacity)) read before
-// any block updates count, and each node's first work item. An inner node
-// with sums is one item (cleared); a leaf with new points one item per
-// kAccumChunk points. Folded-leaf and point totals are counted here.
-__global__ void __launch_bounds__(1024) k_accum_plan(Dev d, int useList) {
-    __shared__ uint32_t s_warp[32];
-    __shared__ uint32_t s_run, s_leaves;
+// The fold's plan: the nodes to visit (the dirty list, or every node), each
+// leaf's new range [count, min(numPoints, capacity)) read before any fold
+// updates count, and each node's work items. An inner node with sums is one
+// item (cleared); a leaf with new points one item per point chunk its new
+// range touches. Sums are exact, so the order of items is free: each block
+// claims a contiguous run of item indices with one atomic (Counters::
+// accumItems, zeroed before the launch) and writes every item's plan entry,
+// so a warp of the fold finds its item with one load. Items can pass
+// accumUnitCap (every live point chunk plus every node) only once the arena
+// has run out (RB_OVF_ARENA): those are not folded. Folded-leaf and point
+// totals are added per block.
+__global__ void __launch_bounds__(256) k_accum_plan(Dev d, int useList) {
+    __shared__ uint32_t s_warp[8];
+    __shared__ uint32_t s_base, s_leaves;
     __shared__ unsigned long long s_points;
     Counters* c = d.ctr;
     const uint32_t total = useList ? (c->numDirty < d.maxNodes ? c->numDirty : d.maxNodes) : c->numNodes;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
-        s_run = 0;
         s_leaves = 0;
         s_points = 0;
     }
     __syncthreads();
-    for (uint32_t w0 = 0; w0 < total; w0 += blockDim.x) {
+    // the same number of steps in every thread of the block
+    for (uint32_t w0 = blockIdx.x * blockDim.x; w0 < total; w0 += gridDim.x * blockDim.x) {
         const uint32_t w = w0 + threadIdx.x;
         uint32_t items = 0, from = 0, to = 0;
         if (w < total) {
@@ -118,7 +119,7 @@ __global__ void __launch_bounds__(1024) k_accum_plan(Dev d, int useList) {
                 const uint32_t np = d.numPoints[node];
                 to = np < cap ? np : cap;
                 if (to > from) {
-                    items = (to - from + kAccumChunk - 1u) / kAccumChunk;
+                    items = (to - 1u) / d.ppc - from / d.ppc + 1u;
                     atomicAdd(&s_leaves, 1u);
                     atomicAdd(&s_points, (unsigned long long)(to - from));
                 } else {
@@ -137,138 +138,145 @@ __global__ void __launch_bounds__(1024) k_accum_plan(Dev d, int useList) {
         }
         if (lane == 31u) s_warp[warp] = x;
         __syncthreads();
-        if (warp == 0) {
-            uint32_t v = lane < blockDim.x / 32u ? s_warp[lane] : 0u;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
-                if (lane >= (uint32_t)o) v += y;
+        if (threadIdx.x == 0) {
+            uint32_t run = 0;
+            for (uint32_t k = 0; k < blockDim.x / 32u; k++) {
+                const uint32_t t = s_warp[k];
+                s_warp[k] = run;
+                run += t;
             }
-            s_warp[lane] = v;
+            s_base = run ? atomicAdd(&c->accumItems, run) : 0u;
         }
         __syncthreads();
-        const uint32_t pre = s_run + (warp > 0 ? s_warp[warp - 1] : 0u) + x - items;
-        if (w < total) d.accumItem[w] = pre;
-        __syncthreads();
-        if (threadIdx.x == 0) s_run += s_warp[blockDim.x / 32u - 1u];
+        const uint32_t first = s_base + s_warp[warp] + x - items;
+        if (w < total) {
+            d.accumItem[w] = first;
+            for (uint32_t u = first; u < first + items && u < d.accumUnitCap; u++) d.accumUnitW[u] = w;
+        }
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        d.accumItem[total] = s_run;
-        c->accumItems = s_run;
-        d.accumGlobals->numAccumulated += s_points;
-        d.accumGlobals->pointsFolded += (uint32_t)s_points;
-        d.accumGlobals->numLeavesFolded += s_leaves;
+    __syncthreads();
+    if (threadIdx.x == 0 && s_leaves) {
+        atomicAdd(&d.accumGlobals->numAccumulated, s_points);
+        atomicAdd(&d.accumGlobals->pointsFolded, (uint32_t)s_points);
+        atomicAdd(&d.accumGlobals->numLeavesFolded, s_leaves);
     }
 }
 
-// Folds the plan's work items: each a kAccumChunk-point slice of one leaf's
-// new range (partial sums added atomically into the leaf's exact sums; any
-// order gives the same bits), or an inner node's sums cleared.
-__global__ void __launch_bounds__(kAccumThreads, 4) k_accumulate(Dev d, uint32_t batchIndex, int useList) {
-    __shared__ unsigned long long s_red[kNumSums][kAccumWarps];
-    __shared__ unsigned long long s_morton[kAccumWarps];
+// 128-bit sum of two (lo, hi) pairs.
+__device__ __forceinline__ void add128pair(unsigned long long& lo, unsigned long long& hi, unsigned long long olo,
+                                           unsigned long long ohi) {
+    const unsigned long long nl = lo + olo;
+    hi += ohi + (nl < lo ? 1ull : 0ull);
+    lo = nl;
+}
+
+// Folds the plan's work items, one warp per item: an item is the part of one
+// leaf's new range inside one point chunk (at most ppc points, one chunk-table
+// read), its partial sums added atomically into the leaf's exact sums -- any
+// order gives the same bits -- or an inner node's sums cleared. Lane k of the
+// warp issues the atomic of sum k, so an item's 21 updates go out together.
+// The watermark is merged per block in shared memory, one global atomic per
+// block.
+__global__ void __launch_bounds__(kAccumThreads) k_accumulate(Dev d, uint32_t batchIndex, int useList) {
+    __shared__ unsigned long long s_morton;
     const Counters* c = d.ctr;
-    const uint32_t total = useList ? (c->numDirty < d.maxNodes ? c->numDirty : d.maxNodes) : c->numNodes;
     const uint32_t items = c->accumItems;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ppc = d.ppc;
-    for (uint32_t it = blockIdx.x; it < items; it += gridDim.x) {
-        // the node whose items hold this one: last w with accumItem[w] <= it
-        uint32_t lo = 0, hi = total;
-        while (hi - lo > 1u) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (d.accumItem[mid] <= it) lo = mid;
-            else hi = mid;
-        }
-        const uint32_t w = lo;
+    if (threadIdx.x == 0) s_morton = 0ull;
+    __syncthreads();
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long blockMax = 0ull;  // lane 0's running watermark
+    for (uint32_t it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items; it += warps) {
+        if (it >= d.accumUnitCap) break;  // only past an arena overflow (see k_accum_plan)
+        const uint32_t w = d.accumUnitW[it];
         const uint32_t node = useList ? d.dirtyList[w] : w;
         AccumI* a = &d.accum[node];
         const uint32_t from0 = d.accumFrom[w], to = d.accumTo[w];
         if (to == from0) {  // an inner node holding sums
-            if (threadIdx.x == 0) {
+            if (lane == 0) {
                 AccumI z = {};
                 *a = z;
             }
             continue;
         }
-        const uint32_t k0 = it - d.accumItem[w];
-        const uint32_t from = from0 + k0 * kAccumChunk;
-        const uint32_t end = min(to, from + kAccumChunk);
+        const uint32_t ci = from0 / ppc + (it - d.accumItem[w]);
+        const uint32_t from = from0 > ci * ppc ? from0 : ci * ppc;
+        const uint32_t end = to < (ci + 1u) * ppc ? to : (ci + 1u) * ppc;
         const uint32_t lv = d.level[node];
         const uint32_t sh = 28u - lv;
         const long long lim = 1ll << sh;
         const long long bx = (long long)d.nodeX[node] << sh;
         const long long by = (long long)d.nodeY[node] << sh;
         const long long bz = (long long)d.nodeZ[node] << sh;
-        const uint32_t toff = d.ptTableOff[node];
+        const uint32_t phys = d.tablePool[d.ptTableOff[node] + ci];
 
-        // Per thread at most kAccumChunk / kAccumThreads = 16 points per item:
-        // Σq < 2^32 · 16 needs u64, Σq·q < 16 · 2^56 fits u64 without carries,
-        // colour sums fit u32; the 128-bit carries start at the warp reduction.
+        // Per lane at most ppc / 32 + 1 points: Σq < 2^28 · 32 needs u64, Σq·q <
+        // 32 · 2^56 fits u64 without carries, colour sums fit u32; the 128-bit
+        // carries start at the warp reduction.
         unsigned long long s1[3] = {0, 0, 0};
         unsigned long long p2[6] = {0, 0, 0, 0, 0, 0};
         uint32_t c1[3] = {0, 0, 0}, c2[3] = {0, 0, 0};
         uint32_t mx = 0, my = 0, mz = 0;  // the largest point in Morton order so far
-        for (uint32_t s0 = from + threadIdx.x; s0 < end; s0 += 2u * blockDim.x) {
-            // two points per step: independent chunk-table and point loads in flight
-            float4 v2[2];
-            bool ok[2];
+        if (phys != kNone) {
+            const float4* cp = reinterpret_cast<const float4*>(chunkPoints(d, phys));
+            const uint32_t base = ci * ppc;
+            for (uint32_t s0 = from + lane; s0 < end; s0 += 4u * 32u) {
+                // four points per step: their loads in flight together
+                float4 v4[4];
+                bool ok[4];
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const uint32_t s = s0 + (uint32_t)h * blockDim.x;
-                ok[h] = false;
-                if (s < end) {
-                    const uint32_t phys = d.tablePool[toff + s / ppc];
-                    if (phys != kNone) {
-                        v2[h] = __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc));
-                        ok[h] = true;
+                for (int h = 0; h < 4; h++) {
+                    const uint32_t sidx = s0 + (uint32_t)h * 32u;
+                    ok[h] = sidx < end;
+                    if (ok[h]) v4[h] = __ldg(cp + (sidx - base));
+                }
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    if (!ok[h]) continue;
+                    const float4 v = v4[h];
+                    const uint32_t P[3] = {aq(v.x, d.boxMin[0], d.octreeSize, 268435456.0f),
+                                           aq(v.y, d.boxMin[1], d.octreeSize, 268435456.0f),
+                                           aq(v.z, d.boxMin[2], d.octreeSize, 268435456.0f)};
+                    // clamped to [0, 2^(28 - level)]: 32-bit values, 64-bit products
+                    uint32_t q[3];
+                    const long long r[3] = {(long long)P[0] - bx, (long long)P[1] - by, (long long)P[2] - bz};
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        q[k] = (uint32_t)(r[k] < 0 ? 0 : (r[k] > lim ? lim : r[k]));
+                        s1[k] += q[k];
+                    }
+                    p2[0] += (unsigned long long)q[0] * q[0];
+                    p2[1] += (unsigned long long)q[0] * q[1];
+                    p2[2] += (unsigned long long)q[0] * q[2];
+                    p2[3] += (unsigned long long)q[1] * q[1];
+                    p2[4] += (unsigned long long)q[1] * q[2];
+                    p2[5] += (unsigned long long)q[2] * q[2];
+                    const uint32_t col = __float_as_uint(v.w);
+                    const uint32_t ch[3] = {col & 255u, (col >> 8) & 255u, (col >> 16) & 255u};
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        c1[k] += ch[k];
+                        c2[k] += ch[k] * ch[k];
+                    }
+                    // the 20-bit coordinate is the 28-bit one shifted (power-of-two scaling
+                    // commutes with round-to-nearest); only a saturated conversion differs
+                    uint32_t X = P[0] < 0xFFFFFF00u ? P[0] >> 8 : aq(v.x, d.boxMin[0], d.octreeSize, 1048576.0f);
+                    uint32_t Y = P[1] < 0xFFFFFF00u ? P[1] >> 8 : aq(v.y, d.boxMin[1], d.octreeSize, 1048576.0f);
+                    uint32_t Z = P[2] < 0xFFFFFF00u ? P[2] >> 8 : aq(v.z, d.boxMin[2], d.octreeSize, 1048576.0f);
+                    X = X < 1048575u ? X : 1048575u;
+                    Y = Y < 1048575u ? Y : 1048575u;
+                    Z = Z < 1048575u ? Z : 1048575u;
+                    if (mortonLess(mx, my, mz, X, Y, Z)) {
+                        mx = X;
+                        my = Y;
+                        mz = Z;
                     }
                 }
             }
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                if (!ok[h]) continue;
-                const float4 v = v2[h];
-                const uint32_t P[3] = {aq(v.x, d.boxMin[0], d.octreeSize, 268435456.0f),
-                                       aq(v.y, d.boxMin[1], d.octreeSize, 268435456.0f),
-                                       aq(v.z, d.boxMin[2], d.octreeSize, 268435456.0f)};
-                // clamped to [0, 2^(28 - level)]: 32-bit values, 64-bit products
-                uint32_t q[3];
-                const long long r[3] = {(long long)P[0] - bx, (long long)P[1] - by, (long long)P[2] - bz};
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    q[k] = (uint32_t)(r[k] < 0 ? 0 : (r[k] > lim ? lim : r[k]));
-                    s1[k] += q[k];
-                }
-                p2[0] += (unsigned long long)q[0] * q[0];
-                p2[1] += (unsigned long long)q[0] * q[1];
-                p2[2] += (unsigned long long)q[0] * q[2];
-                p2[3] += (unsigned long long)q[1] * q[1];
-                p2[4] += (unsigned long long)q[1] * q[2];
-                p2[5] += (unsigned long long)q[2] * q[2];
-                const uint32_t col = __float_as_uint(v.w);
-                const uint32_t ch[3] = {col & 255u, (col >> 8) & 255u, (col >> 16) & 255u};
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    c1[k] += ch[k];
-                    c2[k] += ch[k] * ch[k];
-                }
-                // the 20-bit coordinate is the 28-bit one shifted (power-of-two scaling
-                // commutes with round-to-nearest); only a saturated conversion differs
-                uint32_t X = P[0] < 0xFFFFFF00u ? P[0] >> 8 : aq(v.x, d.boxMin[0], d.octreeSize, 1048576.0f);
-                uint32_t Y = P[1] < 0xFFFFFF00u ? P[1] >> 8 : aq(v.y, d.boxMin[1], d.octreeSize, 1048576.0f);
-                uint32_t Z = P[2] < 0xFFFFFF00u ? P[2] >> 8 : aq(v.z, d.boxMin[2], d.octreeSize, 1048576.0f);
-                X = X < 1048575u ? X : 1048575u;
-                Y = Y < 1048575u ? Y : 1048575u;
-                Z = Z < 1048575u ? Z : 1048575u;
-                if (mortonLess(mx, my, mz, X, Y, Z)) {
-                    mx = X;
-                    my = Y;
-                    mz = Z;
-                }
-            }
         }
+        // the warp's sums: 21 values (s1 x3, s2 lo/hi x6, c1 x3, c2 x3) and the watermark
         unsigned long long wm = (mortonSpread(mx) << 2) | (mortonSpread(my) << 1) | mortonSpread(mz);
         unsigned long long lo2[6], hi2[6] = {0, 0, 0, 0, 0, 0};
         unsigned long long c1w[3], c2w[3];
@@ -279,68 +287,58 @@ __global__ void __launch_bounds__(kAccumThreads, 4) k_accumulate(Dev d, uint32_t
             c1w[k] = c1[k];
             c2w[k] = c2[k];
         }
-        // warp reduction
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
             for (int k = 0; k < 3; k++) {
-                s1[k] += __shfl_down_sync(0xFFFFFFFFu, s1[k], off);
-                c1w[k] += __shfl_down_sync(0xFFFFFFFFu, c1w[k], off);
-                c2w[k] += __shfl_down_sync(0xFFFFFFFFu, c2w[k], off);
+                s1[k] += __shfl_xor_sync(0xFFFFFFFFu, s1[k], off);
+                c1w[k] += __shfl_xor_sync(0xFFFFFFFFu, c1w[k], off);
+                c2w[k] += __shfl_xor_sync(0xFFFFFFFFu, c2w[k], off);
             }
 #pragma unroll
             for (int k = 0; k < 6; k++) {
-                const unsigned long long ol = __shfl_down_sync(0xFFFFFFFFu, lo2[k], off);
-                const unsigned long long oh = __shfl_down_sync(0xFFFFFFFFu, hi2[k], off);
-                const unsigned long long nl = lo2[k] + ol;
-                hi2[k] += oh + (nl < lo2[k] ? 1ull : 0ull);
-                lo2[k] = nl;
+                const unsigned long long ol = __shfl_xor_sync(0xFFFFFFFFu, lo2[k], off);
+                const unsigned long long oh = __shfl_xor_sync(0xFFFFFFFFu, hi2[k], off);
+                add128pair(lo2[k], hi2[k], ol, oh);
             }
-            const unsigned long long om = __shfl_down_sync(0xFFFFFFFFu, wm, off);
+            const unsigned long long om = __shfl_xor_sync(0xFFFFFFFFu, wm, off);
             wm = om > wm ? om : wm;
         }
-        if (lane == 0) {
+        // every lane holds the totals: lane k issues sum k's atomic (values
+        // picked by unrolled selects, so the arrays stay in registers)
+        if (lane < 3u) {
+            unsigned long long v1 = 0, vc1 = 0, vc2 = 0;
+#pragma unroll
             for (int k = 0; k < 3; k++) {
-                s_red[k][warp] = s1[k];
-                s_red[15 + k][warp] = c1w[k];
-                s_red[18 + k][warp] = c2w[k];
+                if (lane == (uint32_t)k) {
+                    v1 = s1[k];
+                    vc1 = c1w[k];
+                    vc2 = c2w[k];
+                }
             }
+            atomicAdd(&a->s1[lane], v1);
+            atomicAdd(&a->c1[lane], vc1);
+            atomicAdd(&a->c2[lane], vc2);
+        } else if (lane < 9u) {
+            unsigned long long vlo = 0, vhi = 0;
+#pragma unroll
             for (int k = 0; k < 6; k++) {
-                s_red[3 + k][warp] = lo2[k];
-                s_red[9 + k][warp] = hi2[k];
-            }
-            s_morton[warp] = wm;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long t1[3] = {0, 0, 0}, tc1[3] = {0, 0, 0}, tc2[3] = {0, 0, 0};
-            unsigned long long tlo[6] = {0, 0, 0, 0, 0, 0}, thi[6] = {0, 0, 0, 0, 0, 0};
-            unsigned long long m = 0;
-            for (int w2 = 0; w2 < kAccumWarps; w2++) {
-                for (int k = 0; k < 3; k++) {
-                    t1[k] += s_red[k][w2];
-                    tc1[k] += s_red[15 + k][w2];
-                    tc2[k] += s_red[18 + k][w2];
+                if (lane == 3u + (uint32_t)k) {
+                    vlo = lo2[k];
+                    vhi = hi2[k];
                 }
-                for (int k = 0; k < 6; k++) {
-                    thi[k] += s_red[9 + k][w2];
-                    add128(tlo[k], thi[k], s_red[3 + k][w2]);
-                }
-                m = s_morton[w2] > m ? s_morton[w2] : m;
             }
-            for (int k = 0; k < 3; k++) {
-                atomicAdd(&a->s1[k], t1[k]);
-                atomicAdd(&a->c1[k], tc1[k]);
-                atomicAdd(&a->c2[k], tc2[k]);
-            }
-            for (int k = 0; k < 6; k++) atomicAdd128(&a->s2lo[k], &a->s2hi[k], tlo[k], thi[k]);
+            atomicAdd128(&a->s2lo[lane - 3u], &a->s2hi[lane - 3u], vlo, vhi);
+        } else if (lane == 9u) {
             // every item of a leaf writes the same watermark and batch
             a->count = to;
             a->lastTouchedBatch = batchIndex;
-            atomicMax(&d.accumGlobals->mortonWatermark, m);
         }
-        __syncthreads();
+        if (wm > blockMax) blockMax = wm;
     }
+    if (lane == 0 && blockMax != 0ull) atomicMax(&s_morton, blockMax);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_morton != 0ull) atomicMax(&d.accumGlobals->mortonWatermark, s_morton);
 }
 
 // kernel_accum_verify (remolod_accum.cu:214-233)
@@ -357,7 +355,8 @@ __global__ void __launch_bounds__(256) k_accum_verify(Dev d) {
 }
 
 void launchAccumulate(const Dev& d, uint32_t batchIndex, int useList, int grid, cudaStream_t s) {
-    k_accum_plan<<<1, 1024, 0, s>>>(d, useList);
+    cudaMemsetAsync(&d.ctr->accumItems, 0, sizeof(uint32_t), s);
+    k_accum_plan<<<grid, 256, 0, s>>>(d, useList);
     k_accumulate<<<grid, kAccumThreads, 0, s>>>(d, batchIndex, useList);
 }
 void launchAccumVerify(const Dev& d, int grid, cudaStream_t s) { k_accum_verify<<<grid, 256, 0, s>>>(d); }

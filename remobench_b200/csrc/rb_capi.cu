@@ -584,6 +584,8 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.accumFrom, N, "accumulate plan ranges");
     ALLOC(d.accumTo, N, "accumulate plan ranges");
     ALLOC(d.accumItem, (uint64_t)N + 1, "accumulate plan items");
+    d.accumUnitCap = (uint32_t)std::min<uint64_t>((uint64_t)d.maxPtChunks + N, UINT32_MAX);
+    ALLOC(d.accumUnitW, d.accumUnitCap, "accumulate work items");
     ALLOC(d.hist8, (uint64_t)N * 8, "child-octant counts");
     ALLOC(d.arrive, N, "points reaching each leaf");
     ALLOC(d.deepCnt, (uint64_t)rb::kDeepRoots * rb::kDeepCells, "expand round bins");

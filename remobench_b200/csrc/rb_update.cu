@@ -1088,7 +1088,7 @@ __global__ void __launch_bounds__(1024) k_deep_book(Dev d) {
 // A block's bin counts, merged in shared memory before they reach the global
 // bins: the coarse cubes (8 per root at depth 1) are shared by most of a
 // batch's points, and one global atomic per warp on them serialises in one L2
-// slice. Keys are bin indices (slot * kDeepCells + cube), below 2^22.
+// slice. Keys are bin indices (slot * kDeepCells + cube), below 2^25.
 constexpr uint32_t kDeepBlockBins = 1024;
 struct DeepBlockBins {
     uint32_t key[kDeepBlockBins];

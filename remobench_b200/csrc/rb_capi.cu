@@ -30,7 +30,7 @@ enum KernelId : int {
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
     K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_PASS, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE,
-    K_EXPAND_REST, K_WIREFRAME, K_REFINE_COLORS, K_ALLOC_VOXELS, K_FINISH_LEAVES, K_NUM
+    K_EXPAND_REST, K_WIREFRAME, K_REFINE_COLORS, K_ALLOC_VOXELS, K_FINISH_LEAVES, K_VOX_LIFT, K_VOX_SAMPLE_LEVELS, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
@@ -41,7 +41,7 @@ static const char* const kKernelNames[K_NUM] = {
     "k_expand_cond", "k_zero_grids",
     // not a kernel: per-iteration expand passes run inside k_expand_rest
     "expand_pass", "k_deep_book", "k_deep_bin", "k_deep_split", "k_deep_move", "k_expand_rest",
-    "k_wireframe", "k_refine_colors", "k_alloc_voxels", "k_finish_leaves"};
+    "k_wireframe", "k_refine_colors", "k_alloc_voxels", "k_finish_leaves", "k_vox_lift", "k_vox_sample_levels"};
 
 struct Profiler {
     bool on = false;
@@ -255,6 +255,8 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
     LAUNCH(c, K_ZERO_GRIDS, 0, rb::launchZeroGrids(d, fixedGrid, s));
     LAUNCH(c, K_FINISH_LEAVES, n, rb::launchFinishLeaves(d, pts, n, pointGrid(c, work), s));
     LAUNCH(c, K_VOX_SAMPLE, n, rb::launchVoxSample(d, pts, n, pointGrid(c, work), s));
+    LAUNCH(c, K_VOX_SAMPLE_LEVELS, n, rb::launchVoxSampleLevels(d, pts, n, pointGrid(c, work), s));
+    LAUNCH(c, K_VOX_LIFT, 0, rb::launchVoxLift(d, pointGrid(c, work), s));
     // four blocks per SM: fewer blocks, fewer reservations on a node's voxel counter
     LAUNCH(c, K_VOX_COMMIT, 0, rb::launchVoxCommit(d, fixedGrid, s));
     LAUNCH(c, K_ALLOC_VOXELS, 0, rb::launchAllocVoxels(d, fixedGrid, s));
@@ -283,14 +285,14 @@ bool graphPath(rb_ctx* c) {
     return c->batchGraph != nullptr;
 }
 
-// Launches of graph batches, for the per-kernel counts: fourteen kernels per
+// Launches of graph batches, for the per-kernel counts: sixteen kernels per
 // batch (k_expand_rest zeroes the split grids and finishes the leaves); the
 // per-iteration passes k_expand_rest ran (one loop test each) are counted as
 // expand_pass, not as launches.
 void countGraphLaunches(rb_ctx* c, uint64_t batches, uint32_t condBefore, uint64_t points) {
     const uint32_t passes = c->hostCtr->condRuns - condBefore;
     for (int k : {K_BATCH_BEGIN, K_COUNT_FIRST, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE, K_EXPAND_REST,
-                  K_VOX_SAMPLE, K_VOX_COMMIT, K_ALLOC_VOXELS, K_VOX_STORE, K_ALLOC_POINTS, K_INSERT,
+                  K_VOX_SAMPLE, K_VOX_SAMPLE_LEVELS, K_VOX_LIFT, K_VOX_COMMIT, K_ALLOC_VOXELS, K_VOX_STORE, K_ALLOC_POINTS, K_INSERT,
                   K_BATCH_END})
         c->prof.launches[k] += batches;
     c->prof.launches[K_EXPAND_PASS] += passes;

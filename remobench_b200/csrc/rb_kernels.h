@@ -48,6 +48,8 @@ void launchDeepMove(const Dev& d, const Point* pts, uint32_t n, int grid, cudaSt
 void launchExpandCond(const Dev& d, cudaStream_t s);
 void launchSpillCopy(const Dev& d, int grid, cudaStream_t s);
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
+void launchVoxLift(const Dev& d, int grid, cudaStream_t s);
+void launchVoxSampleLevels(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchVoxCommit(const Dev& d, int grid, cudaStream_t s);
 void launchFinishLeaves(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchAllocPoints(const Dev& d, int grid, cudaStream_t s);

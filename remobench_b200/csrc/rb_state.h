@@ -55,11 +55,14 @@ struct Counters {
     uint32_t numSplit;            // nodes split by the last split
     uint32_t numSpilled;          // spilled points this batch
     uint32_t numNew;              // new voxel cells this batch
+    uint32_t numLift;             // new voxel cells k_vox_lift listed after numNew
+    uint32_t levelMode;           // this batch samples voxels level by level (gridsPartial at its start)
     uint32_t spillChunkTotal;     // copy work items of the last split
     uint32_t loopMore;            // the last loop test's answer: another expand pass
     // flags and diagnostics (sticky until reset)
     uint32_t memCapacityReached;
     uint32_t nodePoolOverflow;
+    uint32_t gridsPartial;        // a batch lost new cells to a full list: later batches sample level by level
     uint32_t overflowFlags;       // RB_OVF_* bits
     uint32_t condSkips;           // unrolled expand passes skipped after the loop ended (wraps)
     uint64_t droppedPoints;

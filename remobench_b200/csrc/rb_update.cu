@@ -232,6 +232,8 @@ __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     c->numSpill = 0;
     c->numSpilled = 0;
     c->numNew = 0;
+    c->numLift = 0;
+    c->levelMode = c->gridsPartial;
     c->numSplit = 0;
     c->spillChunkTotal = 0;
     c->iter = 1;
@@ -1491,6 +1493,7 @@ __device__ __forceinline__ void listNewCell(const Dev& d, uint32_t e, uint32_t s
     } else {
         atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
         d.ctr->hashNeedsClear = 1u;
+        d.ctr->gridsPartial = 1u;
     }
 }
 
@@ -1520,6 +1523,7 @@ __device__ void hashInsertFrom(const Dev& d, unsigned long long key, unsigned lo
     }
     atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
     d.ctr->hashNeedsClear = 1u;
+    d.ctr->gridsPartial = 1u;
 }
 
 __device__ __forceinline__ uint32_t cellAt(uint32_t x28, uint32_t y28, uint32_t z28, uint32_t level) {
@@ -1527,16 +1531,14 @@ __device__ __forceinline__ uint32_t cellAt(uint32_t x28, uint32_t y28, uint32_t 
     return ((x28 >> sh) & 127u) + ((y28 >> sh) & 127u) * 128u + ((z28 >> sh) & 127u) * 16384u;
 }
 
-constexpr uint32_t kInsertGroup = 4;  // table updates a lane keeps in flight
 // Per-block cache of cells this block's points lead, direct-mapped: entry
 // (tag << 32) | global point index, tag = key >> kCellCacheBits (under 2^31,
 // since node ids stay below 2^21), position = the key's low bits plus a hash of
 // the tag, so tag and position give back the key.
 constexpr uint32_t kCellCacheBits = 11;
 constexpr uint32_t kCellCache = 1u << kCellCacheBits;
-// Per-warp buffer of claimed table slots: under 32 waiting plus one group of
-// at most 32 lanes x kInsertGroup claims.
-constexpr uint32_t kWarpCells = 32u + 32u * kInsertGroup;
+// Per-warp buffer of claimed table slots: under 32 waiting plus one claim per lane.
+constexpr uint32_t kWarpCells = 64u;
 
 // The warp's buffered slots into the batch's list of new cells, with one
 // counter atomic (a single counter bumped by every claim serialises the
@@ -1551,8 +1553,234 @@ __device__ __forceinline__ void flushWarpCells(const Dev& d, const uint32_t* wbu
     __syncwarp();
 }
 
-// voxelSampling (remolod_octree.cu:677-740) + sampleVoxel's test (:95-119):
-// every (point, level) pair whose cell bit was clear before this batch is a
+// voxelSampling (remolod_octree.cu:677-740) + sampleVoxel's test (:95-119),
+// first half. A point tests the cell of every node on its path whose grid
+// exists: the ancestors of its leaf, and the leaf itself while it has a grid
+// (a root that has never split). Its cell in node N at level l is the top
+// 7 + l bits of its 28-bit coordinates, so its cells on the path are prefixes
+// of its cell at the deepest tested level D; and a bit is only ever set
+// together with the same point's bits at every level above (a grid is zeroed
+// when its node splits, before any node below it exists). So the levels whose
+// cell was empty before this batch are a run ending at D, and the point's
+// whole contribution follows from one test: its cell at D. When that bit is
+// clear, the cell goes into the batch's table, which keeps per cell the lowest
+// global point index reaching it (or the first to arrive); k_vox_lift then
+// carries every new cell's representative up to the levels above. The set of
+// new cells and their representatives are exactly the per-level sampling's.
+//
+// Bits are not written here, so every point sees the pre-batch grids. One
+// leader per run of equal cells in the warp (batch points ascend in index with
+// the lane, so a run's first lane holds its lowest index; spilled points use a
+// full match), then a per-block direct-mapped cache drops a leader whose cell
+// an earlier point of the block already leads (a lower index, or any point in
+// first-come mode). Claimed slots are buffered per warp and listed 32 at a
+// time with one counter atomic.
+__global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    __shared__ uint32_t s_wbuf[256 / 32][kWarpCells];
+    __shared__ unsigned long long s_cells[kCellCache];
+    const Counters* c = d.ctr;
+    if (c->batchStop || c->levelMode) return;
+    for (uint32_t t = threadIdx.x; t < kCellCache; t += blockDim.x) s_cells[t] = ~0ull;
+    __syncthreads();
+    // single 64-bit accesses: an entry is read and written whole
+    volatile unsigned long long* cells = s_cells;
+    RB_BATCH_AT_CURSOR(d, pts, n);
+    uint32_t* wbuf = s_wbuf[threadIdx.x >> 5];
+    uint32_t wbufN = 0;  // the same in every lane of the warp
+    const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
+    const uint32_t total = n + ns;
+    const uint32_t firstIndex = (uint32_t)c->numPointsProcessed;
+    const bool lowest = d.voxelMode == 0u;
+    const uint32_t lane = laneId();
+    const uint32_t per = (((total + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
+    const uint32_t begin = min(total, blockIdx.x * per), end = min(total, begin + per);
+    for (uint32_t base = begin; base < end; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const bool active = i < end;
+        Point p = {0.f, 0.f, 0.f, 0u};
+        uint32_t gidx = 0, leaf = 0;
+        if (active && i < n) {
+            p = loadPoint(pts + i);
+            gidx = firstIndex + i;
+            leaf = d.leafOf[i];
+        } else if (active) {
+            p = d.spillPts[i - n];
+            gidx = d.spillIdx[i - n];
+            leaf = d.spillLeaf[i - n];
+        }
+        // the deepest tested node: the leaf while it has a grid, else its parent
+        unsigned long long key = kHashEmpty;
+        if (active) {
+            const uint32_t lv = d.level[leaf];
+            uint32_t node = leaf, g = d.grid[leaf], tl = lv;
+            if (g == kNone && lv > 0u) {
+                const uint2 a = d.anc[(size_t)leaf * kMaxDepth + lv - 1u];
+                node = a.x;
+                g = a.y;
+                tl = lv - 1u;
+            }
+            if (g != kNone) {
+                const uint32_t x28 = quant28(p.x, d.boxMin[0], d.octreeSize);
+                const uint32_t y28 = quant28(p.y, d.boxMin[1], d.octreeSize);
+                const uint32_t z28 = quant28(p.z, d.boxMin[2], d.octreeSize);
+                const uint32_t vi = cellAt(x28, y28, z28, tl);
+                if (((__ldg(gridWordsAt(d, g) + (vi >> 5)) >> (vi & 31u)) & 1u) == 0u)
+                    key = ((unsigned long long)node << 21) | (unsigned long long)vi;
+            }
+        }
+        // one leader per cell in the warp
+        bool first;
+        if (__all_sync(0xFFFFFFFFu, !active || i < n)) {
+            const unsigned long long prev = __shfl_up_sync(0xFFFFFFFFu, key, 1);
+            first = key != kHashEmpty && (lane == 0u || prev != key);
+        } else {
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+            if (lowest) first = key != kHashEmpty && gidx == __reduce_min_sync(peers, gidx);
+            else first = key != kHashEmpty && lane == (uint32_t)(__ffs(peers) - 1);
+        }
+        if (first) {
+            const uint32_t tag = (uint32_t)(key >> kCellCacheBits);
+            const uint32_t e = ((uint32_t)key + ((tag * 0x9E3779B1u) >> (32u - kCellCacheBits))) & (kCellCache - 1u);
+            const unsigned long long held = cells[e];
+            if ((uint32_t)(held >> 32) == tag && (!lowest || (uint32_t)held < gidx)) first = false;
+            else cells[e] = ((unsigned long long)tag << 32) | gidx;
+        }
+        // the leader's table update: read, claim an empty slot, lower the index
+        bool claimed = false;
+        uint32_t slot = 0;
+        if (first) {
+            const unsigned long long val = ((unsigned long long)gidx << 32) | p.color;
+            slot = hashSlot(key, d.hashMask);
+            const ulonglong2 kv = __ldcg(&d.hashSlots[slot]);
+            unsigned long long cur = kv.x;
+            bool update = false;
+            if (cur == key) {
+                update = lowest ? kv.y > val : kv.y == kHashEmpty;
+            } else if (cur == kHashEmpty) {
+                cur = atomicCAS(&d.hashSlots[slot].x, kHashEmpty, key);
+                claimed = cur == kHashEmpty;
+                update = claimed || cur == key;
+                if (!update) hashInsertFrom(d, key, val, (slot + 1u) & d.hashMask);
+            } else {
+                hashInsertFrom(d, key, val, (slot + 1u) & d.hashMask);
+            }
+            if (update) {
+                if (lowest) atomicMin(&d.hashSlots[slot].y, val);
+                else atomicCAS(&d.hashSlots[slot].y, kHashEmpty, val);
+            }
+        }
+        // claimed slots wait in the warp's buffer; 32 or more go to the list of
+        // new cells with one counter atomic
+        const unsigned cm = __ballot_sync(0xFFFFFFFFu, claimed);
+        if (claimed) wbuf[wbufN + (uint32_t)__popc(cm & ((1u << lane) - 1u))] = slot;
+        __syncwarp();
+        wbufN += (uint32_t)__popc(cm);
+        if (wbufN >= 32u) {
+            flushWarpCells(d, wbuf, wbufN);
+            wbufN = 0;
+        }
+    }
+    flushWarpCells(d, wbuf, wbufN);
+}
+
+// Inserts (key -> val) for k_vox_lift. Returns whether the walk goes on: it
+// stops where the cell already holds a lower index (lowest mode) or any point
+// (first-come mode), since that point's own walk carries it further up. Cells
+// it claims go to the block's list (s_list, s_n).
+__device__ __forceinline__ bool liftInsert(const Dev& d, unsigned long long key, unsigned long long val,
+                                           uint32_t* s_list, uint32_t* s_n) {
+    const bool lowest = d.voxelMode == 0u;
+    uint32_t slot = hashSlot(key, d.hashMask);
+    for (uint32_t probe = 0; probe < 256u; probe++) {
+        const ulonglong2 kv = __ldcg(&d.hashSlots[slot]);
+        unsigned long long cur = kv.x;
+        if (cur == key) {
+            if (lowest) return kv.y > val && atomicMin(&d.hashSlots[slot].y, val) > val;
+            return kv.y == kHashEmpty && atomicCAS(&d.hashSlots[slot].y, kHashEmpty, val) == kHashEmpty;
+        }
+        if (cur == kHashEmpty) {
+            cur = atomicCAS(&d.hashSlots[slot].x, kHashEmpty, key);
+            if (cur == kHashEmpty) {
+                s_list[atomicAdd(s_n, 1u)] = slot;
+                if (lowest) return atomicMin(&d.hashSlots[slot].y, val) > val;
+                return atomicCAS(&d.hashSlots[slot].y, kHashEmpty, val) == kHashEmpty;
+            }
+            if (cur == key) {
+                if (lowest) return atomicMin(&d.hashSlots[slot].y, val) > val;
+                return atomicCAS(&d.hashSlots[slot].y, kHashEmpty, val) == kHashEmpty;
+            }
+        }
+        slot = (slot + 1u) & d.hashMask;
+    }
+    atomicOr(&d.ctr->overflowFlags, (uint32_t)kOvfBacklog);
+    d.ctr->hashNeedsClear = 1u;
+    d.ctr->gridsPartial = 1u;
+    return false;
+}
+
+constexpr uint32_t kLiftThreads = 256;
+
+// voxelSampling's second half: every cell k_vox_sample listed carries its
+// representative up its node's ancestors. At each level above, its prefix
+// cell is a new cell of this batch exactly when that cell's bit was clear
+// before the batch (the bits are still the pre-batch ones here), and its
+// representative is the lowest index over the cells below it; a walk stops at
+// the first set bit, or where a lower index is already in place. Cells the
+// walks claim are listed after k_vox_sample's, through a second counter
+// (numLift), one block reservation per pass; a walk claims at most one cell
+// per level, so a pass's claims fit kLiftThreads x kMaxDepth entries.
+__global__ void __launch_bounds__(kLiftThreads) k_vox_lift(Dev d) {
+    __shared__ uint32_t s_list[kLiftThreads * kMaxDepth];
+    __shared__ uint32_t s_n, s_base;
+    const Counters* c = d.ctr;
+    if (c->batchStop || c->levelMode) return;
+    const uint32_t walkers = c->numNew < d.newCap ? c->numNew : d.newCap;
+    const uint32_t listed = c->numNew;
+    for (uint32_t b = blockIdx.x * kLiftThreads; b < walkers; b += gridDim.x * kLiftThreads) {
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        const uint32_t e = b + threadIdx.x;
+        if (e < walkers) {
+            const uint32_t slot = d.hashNew[e];
+            const ulonglong2 kv = __ldcg(&d.hashSlots[slot]);
+            const uint32_t node = (uint32_t)(kv.x >> 21), vi = (uint32_t)(kv.x & 0x1FFFFFull);
+            const uint32_t lv = d.level[node];
+            // the cell's coordinates at 7 + lv bits per axis
+            const uint32_t px = (d.nodeX[node] << 7) | (vi & 127u);
+            const uint32_t py = (d.nodeY[node] << 7) | ((vi >> 7) & 127u);
+            const uint32_t pz = (d.nodeZ[node] << 7) | (vi >> 14);
+            const uint2* row = d.anc + (size_t)node * kMaxDepth;
+            for (uint32_t l = lv; l-- > 0u;) {
+                const uint2 a = row[l];
+                if (a.y == kNone) break;
+                const uint32_t sh = lv - l;
+                const uint32_t cl = ((px >> sh) & 127u) + ((py >> sh) & 127u) * 128u + ((pz >> sh) & 127u) * 16384u;
+                if ((__ldg(gridWordsAt(d, a.y) + (cl >> 5)) >> (cl & 31u)) & 1u) break;
+                if (!liftInsert(d, ((unsigned long long)a.x << 21) | cl, kv.y, s_list, &s_n)) break;
+            }
+        }
+        __syncthreads();
+        const uint32_t cnt = s_n;
+        if (threadIdx.x == 0 && cnt) s_base = atomicAdd(&d.ctr->numLift, cnt);
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < cnt; t += kLiftThreads) {
+            // listed after k_vox_sample's cells: positions listed + numLift
+            const unsigned long long pos = (unsigned long long)listed + s_base + t;
+            listNewCell(d, pos < 0xFFFFFFFFull ? (uint32_t)pos : 0xFFFFFFFFu, s_list[t]);
+        }
+    }
+}
+
+// The level-by-level form of voxel sampling, for the batches after one whose
+// new cells outran the list (Counters::gridsPartial, until the next reset).
+// Cells a full list dropped keep their bits clear while cells below them may
+// have been set, so a clear bit no longer follows from the deepest tested
+// level and k_vox_sample's single test would miss them; this form tests every
+// level on its own and finds every lost cell again.
+constexpr uint32_t kInsertGroup = 4;  // table updates a lane keeps in flight
+constexpr uint32_t kWarpCellsLevels = 32u + 32u * kInsertGroup;
+
+// Every (point, level) pair whose cell bit was clear before this batch is a
 // candidate; the table keeps, per cell, the lowest global point index reaching
 // it (or the first to arrive). Bits are not written here, so every pair sees
 // the pre-batch grid, and the set of new cells is exactly the reference's.
@@ -1569,11 +1797,11 @@ __device__ __forceinline__ void flushWarpCells(const Dev& d, const uint32_t* wbu
 // an earlier point of the same block already leads (a lower index, or any
 // point in first-come mode) drops out: that point's update keeps the table's
 // result, and most of a block's leaders repeat cells its other warps lead.
-__global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restrict__ pts, uint32_t n) {
-    __shared__ uint32_t s_wbuf[256 / 32][kWarpCells];
+__global__ void __launch_bounds__(256) k_vox_sample_levels(Dev d, const Point* __restrict__ pts, uint32_t n) {
+    __shared__ uint32_t s_wbuf[256 / 32][kWarpCellsLevels];
     __shared__ unsigned long long s_cells[kCellCache];
     const Counters* c = d.ctr;
-    if (c->batchStop) return;
+    if (c->batchStop || !c->levelMode) return;
     for (uint32_t t = threadIdx.x; t < kCellCache; t += blockDim.x) s_cells[t] = ~0ull;
     __syncthreads();
     // single 64-bit accesses: an entry is read and written whole
@@ -1743,6 +1971,12 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
     flushWarpCells(d, wbuf, wbufN);
 }
 
+// The new cells both halves of voxel sampling listed, at most the list's capacity.
+__device__ __forceinline__ uint32_t newCellCount(const Dev& d) {
+    const unsigned long long t = (unsigned long long)d.ctr->numNew + d.ctr->numLift;
+    return t < d.newCap ? (uint32_t)t : d.newCap;
+}
+
 // blockReserve for kEntriesPerThread keys per thread at once: every key's
 // count merges into the block table first, then one barrier pair hands out
 // the global reservations. Every thread of the block calls it. Kernels that
@@ -1803,7 +2037,7 @@ __global__ void __launch_bounds__(256) k_vox_commit(Dev d) {
     if (c->batchStop) return;
     blockSlotsInit(s_slots);
     __syncthreads();
-    const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
+    const uint32_t nnew = newCellCount(d);
     const uint32_t per = (((nnew + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
     const uint32_t begin = min(nnew, blockIdx.x * per), end = min(nnew, begin + per);
     for (uint32_t base = begin; base < end; base += blockDim.x * kEntriesPerThread) {
@@ -2039,7 +2273,7 @@ __global__ void __launch_bounds__(256) k_insert(Dev d, const Point* __restrict__
 __global__ void __launch_bounds__(256) k_vox_store(Dev d) {
     const Counters* c = d.ctr;
     if (c->batchStop) return;
-    const uint32_t nnew = c->numNew < d.newCap ? c->numNew : d.newCap;
+    const uint32_t nnew = newCellCount(d);
     const uint32_t ppc = d.ppc;
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nnew; e += gridDim.x * blockDim.x) {
         const uint32_t node = d.hashNewNode[e];
@@ -2197,6 +2431,10 @@ cudaError_t launchExpandRest(const Dev& d, int grid, cudaStream_t s) {
 void launchVoxSample(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_vox_sample<<<grid, 256, 0, s>>>(d, pts, n);
 }
+void launchVoxLift(const Dev& d, int grid, cudaStream_t s) { k_vox_lift<<<grid, kLiftThreads, 0, s>>>(d); }
+void launchVoxSampleLevels(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
+    k_vox_sample_levels<<<grid, 256, 0, s>>>(d, pts, n);
+}
 void launchVoxCommit(const Dev& d, int grid, cudaStream_t s) { k_vox_commit<<<grid, 256, 0, s>>>(d); }
 void launchFinishLeaves(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_finish_leaves<<<grid, 256, 0, s>>>(d, pts, n);
@@ -2214,7 +2452,8 @@ void launchResetRoot(const Dev& d, int grid, cudaStream_t s) { k_reset_root<<<gr
 // One batch as a CUDA graph: the phase kernels of runBatch, every kernel
 // reading its batch from the device cursor, the expand round's leftovers in
 // the cooperative k_expand_rest. After it the graph forks: the voxel path
-// (k_vox_sample, k_vox_commit, k_alloc_voxels, k_vox_store) and the point path
+// (k_vox_sample or, after a lost cell, k_vox_sample_levels; k_vox_lift,
+// k_vox_commit, k_alloc_voxels, k_vox_store) and the point path
 // (k_alloc_points, k_insert) read the finished tree and write disjoint node
 // fields and chunks, so the point path runs in the voxel path's shadow; they
 // join before k_batch_end. One graph launch builds the batch at batchletIndex
@@ -2246,6 +2485,8 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int re
         k_insert<<<pointGrid, 256, 0, cs2>>>(d, nullptr, 0u);
         if ((e = cudaEventRecord(join, cs2)) != cudaSuccess) break;
         k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        k_vox_sample_levels<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        k_vox_lift<<<pointGrid, kLiftThreads, 0, cs>>>(d);
         k_vox_commit<<<fixedGrid, 256, 0, cs>>>(d);
         k_alloc_voxels<<<fixedGrid, 256, 0, cs>>>(d);
         k_vox_store<<<fixedGrid, 256, 0, cs>>>(d);

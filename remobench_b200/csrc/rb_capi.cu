@@ -561,6 +561,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.vxTableCap, N, "voxel table capacities");
     ALLOC(d.splitIter, N, "split stamps");
     ALLOC(d.anc, (uint64_t)N * rb::kMaxDepth, "ancestor table");
+    ALLOC(d.parent, N, "parent table");
     ALLOC(d.dirtyStamp, N, "dirty stamps");
     ALLOC(d.accum, N, "accumulators");
     ALLOC(d.dirtyList, N, "dirty list");

@@ -202,6 +202,7 @@ struct Dev {
     // ancestors are inner then and keep their grids), so one row gives every
     // grid a point of n must test, with no pointer chase.
     uint2* anc;              // [maxNodes * kMaxDepth]
+    uint2* parent;           // [maxNodes] (id, grid) of the parent: row n of anc at level(n) - 1
     uint32_t* dirtyStamp;
     AccumI* accum;
     // storage: one arena in 16-byte units holding grids (256 KB), point chunks

@@ -706,6 +706,7 @@ __device__ __forceinline__ void splitBody(const Dev& d, uint32_t stamp, uint32_t
         for (uint32_t l = 0; l < (uint32_t)kMaxDepth; l++)
             if (l + 1u < lv) crow[l] = prow[l];
         crow[lv - 1u] = make_uint2(node, info.grid);
+        d.parent[ch] = make_uint2(node, info.grid);
         d.child[node * 8u + i] = (int32_t)ch;
     }
     // Round two: with the octant counts known, the children over the limit are
@@ -808,6 +809,7 @@ __device__ __forceinline__ void splitBody(const Dev& d, uint32_t stamp, uint32_t
             for (uint32_t l = 0; l < (uint32_t)kMaxDepth; l++)
                 if (l + 1u < lv) crow[l] = prow[l];
             crow[lv - 1u] = make_uint2(node, info.grid);
+            d.parent[ch] = make_uint2(node, info.grid);
             d.child[node * 8u + i] = (int32_t)ch;
         }
     }
@@ -934,6 +936,7 @@ __device__ __forceinline__ void makeChild(const Dev& d, uint32_t ch, uint32_t pa
     for (uint32_t l = 0; l < (uint32_t)kMaxDepth; l++)
         if (l + 1u < lv) crow[l] = prow[l];
     crow[lv - 1u] = make_uint2(parent, pg);
+    d.parent[ch] = make_uint2(parent, pg);
     d.child[parent * 8u + i] = (int32_t)ch;
 }
 
@@ -1611,10 +1614,11 @@ __global__ void __launch_bounds__(256) k_vox_sample(Dev d, const Point* __restri
         // the deepest tested node: the leaf while it has a grid, else its parent
         unsigned long long key = kHashEmpty;
         if (active) {
+            // level, grid and parent in one round of loads
             const uint32_t lv = d.level[leaf];
             uint32_t node = leaf, g = d.grid[leaf], tl = lv;
+            const uint2 a = lv > 0u ? d.parent[leaf] : make_uint2(kNone, kNone);
             if (g == kNone && lv > 0u) {
-                const uint2 a = d.anc[(size_t)leaf * kMaxDepth + lv - 1u];
                 node = a.x;
                 g = a.y;
                 tl = lv - 1u;
@@ -1719,6 +1723,7 @@ __device__ __forceinline__ bool liftInsert(const Dev& d, unsigned long long key,
 }
 
 constexpr uint32_t kLiftThreads = 256;
+constexpr uint32_t kLiftChunk = 4;  // ancestor levels a walk loads at once
 
 // voxelSampling's second half: every cell k_vox_sample listed carries its
 // representative up its node's ancestors. At each level above, its prefix
@@ -1750,13 +1755,32 @@ __global__ void __launch_bounds__(kLiftThreads) k_vox_lift(Dev d) {
             const uint32_t py = (d.nodeY[node] << 7) | ((vi >> 7) & 127u);
             const uint32_t pz = (d.nodeZ[node] << 7) | (vi >> 14);
             const uint2* row = d.anc + (size_t)node * kMaxDepth;
-            for (uint32_t l = lv; l-- > 0u;) {
-                const uint2 a = row[l];
-                if (a.y == kNone) break;
-                const uint32_t sh = lv - l;
-                const uint32_t cl = ((px >> sh) & 127u) + ((py >> sh) & 127u) * 128u + ((pz >> sh) & 127u) * 16384u;
-                if ((__ldg(gridWordsAt(d, a.y) + (cl >> 5)) >> (cl & 31u)) & 1u) break;
-                if (!liftInsert(d, ((unsigned long long)a.x << 21) | cl, kv.y, s_list, &s_n)) break;
+            // the ancestors and their grid words four levels at a time, then
+            // the table updates one level after another
+            bool go = true;
+            for (uint32_t top = lv; go && top > 0u;) {
+                const uint32_t cnt = top < kLiftChunk ? top : kLiftChunk;
+                uint2 an[kLiftChunk];
+                uint32_t cl[kLiftChunk], word[kLiftChunk];
+#pragma unroll
+                for (uint32_t k = 0; k < kLiftChunk; k++)
+                    an[k] = k < cnt ? row[top - 1u - k] : make_uint2(kNone, kNone);
+#pragma unroll
+                for (uint32_t k = 0; k < kLiftChunk; k++) {
+                    const uint32_t sh = k + 1u + (lv - top);
+                    cl[k] = ((px >> sh) & 127u) + ((py >> sh) & 127u) * 128u + ((pz >> sh) & 127u) * 16384u;
+                    word[k] = an[k].y != kNone ? __ldg(gridWordsAt(d, an[k].y) + (cl[k] >> 5)) : ~0u;
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kLiftChunk; k++) {
+                    if (!go || k >= cnt) break;
+                    if ((word[k] >> (cl[k] & 31u)) & 1u) {
+                        go = false;
+                        break;
+                    }
+                    go = liftInsert(d, ((unsigned long long)an[k].x << 21) | cl[k], kv.y, s_list, &s_n);
+                }
+                top -= cnt;
             }
         }
         __syncthreads();

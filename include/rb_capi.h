@@ -390,6 +390,30 @@ typedef struct rb_refine_result {
 } rb_refine_result;
 rb_status rb_refine_colors(struct rb_ctx* ctx, uint32_t budget, rb_refine_result* out);
 
+/* Refinement's deepening (wiki/02_KernelPipeline.md:228-243, "local split and
+ * redistribute"; the reference lists it, unbuilt): among the first `budget`
+ * nodes of the last Analysis queue, every leaf above the deepest level
+ * (level < 20) holding at least min_points points (0 counts as 1) is split as doSplitting splits a spilling node
+ * (remolod_octree.cu:303-400): in increasing id, 8 consecutive ids each, a
+ * grid (allocated once, zeroed), its points to the new children and its
+ * chunks back to the queue. Voxel sampling then gives the deepened node its
+ * voxels (the lowest global point index per cell) and insertion places the
+ * points. The node pool guard refuses a split once fewer than 8 ids remain
+ * and raises the node-pool flag, as a batch does; the memory check of a
+ * batch refuses the whole pass (stopped, memCapacityReached). No batch is
+ * consumed. Accumulate runs after it when the pipeline has Accumulate. The
+ * Analysis queue is stale afterwards: call rb_analyze before the next
+ * refinement call. */
+typedef struct rb_deepen_result {
+    uint32_t nodes_selected;   /* queue leaves with at least min_points points */
+    uint32_t nodes_split;      /* splits made, the selected leaves the pool had room for first */
+    uint32_t nodes_refused;    /* selected leaves the node pool had no room for */
+    uint32_t stopped;          /* 1: the memory check refused the pass */
+    uint64_t points_moved;     /* stored points redistributed to the new children */
+    uint64_t voxels_made;      /* new voxels sampled for the deepened nodes */
+} rb_deepen_result;
+rb_status rb_refine_deepen(struct rb_ctx* ctx, uint32_t budget, uint32_t min_points, rb_deepen_result* out);
+
 /* The learned scorer (no reference counterpart: plans/04_NeuralPass.md is
  * empty): a 16 -> 64 -> 64 -> 2 MLP, GELU, BF16 weights and activations, FP32
  * accumulation, trained on the GPU with these entry points. Inputs are the 16

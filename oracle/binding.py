@@ -195,6 +195,8 @@ def lib():
         L.or_wireframe.argtypes = [vp, ctypes.POINTER(Frame), vp, vp, u32]
         L.or_features.argtypes = [vp, u32, u32, vp]
         L.or_refine_colors.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
+        L.or_deepen.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u32)]
+        L.or_deepen.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -308,6 +310,14 @@ class Tree:
         m, v = ctypes.c_uint32(), ctypes.c_uint64()
         lib().or_refine_colors(self.h, _ptr(arr), len(arr), capacity, ctypes.byref(m), ctypes.byref(v))
         return m.value, v.value
+
+    def deepen(self, nodes, min_points=0):
+        """Refinement's deepening of the leaves among `nodes`; (refused by the
+        memory check, leaves taken)."""
+        arr = np.ascontiguousarray(nodes, dtype=np.uint32)
+        m = ctypes.c_uint32()
+        rc = lib().or_deepen(self.h, _ptr(arr), len(arr), min_points, ctypes.byref(m))
+        return rc != 0, m.value
 
     def accumulate(self, batch_index):
         g = AccumGlobals()

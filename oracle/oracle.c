@@ -557,26 +557,10 @@ static void insert_at(or_tree* t, uint32_t leaf, const or_point* p, uint32_t ind
     n->idx[slot] = index;
 }
 
-int or_add_batch(or_tree* t, const or_point* pts, uint32_t n) {
-    /* remolod_octree.cu:1181-1210 */
-    if (t->st.persistent_offset + t->cfg.safety_margin >= t->cfg.persistent_capacity) {
-        t->st.mem_capacity_reached = 1;
-        return 1;
-    }
-    t->st.mem_capacity_reached = 0;
-    const uint32_t batch_index = t->st.batchlet_index;
-    const uint32_t first_index = (uint32_t)t->st.num_points_processed;
-    t->spill_n = 0;
-
-    uint32_t* fresh_tag = (uint32_t*)calloc(t->cfg.max_nodes, sizeof(uint32_t));
-    if (!fresh_tag) abort();
-    /* nodes that exist count with countIteration = batchIndex (set in the previous batch) */
-    for (uint32_t i = 0; i < t->num_nodes; i++) fresh_tag[i] = batch_index;
-    expand(t, pts, n, batch_index, fresh_tag);
-    free(fresh_tag);
-    t->st.spilled_points += t->spill_n;
-
-    /* spilled points in increasing original index, then the batch in order */
+/* After expand: voxel sampling (spilled points by original index, then the
+ * batch), chunk allocation, insertPoints and insertVoxels (addBatch's later
+ * phases, remolod_octree.cu:940-1060). */
+static void place_batch(or_tree* t, const or_point* pts, uint32_t n, uint32_t first_index) {
     qsort(t->spill, t->spill_n, sizeof(spill_pt), cmp_spill);
     vbacklog bl = {NULL, 0, 0};
     sample_all(t, pts, n, &bl);
@@ -609,9 +593,99 @@ int or_add_batch(or_tree* t, const or_point* pts, uint32_t n) {
         if (slot < nd->num_voxel_chunks * t->cfg.points_per_chunk) nd->vox[slot] = bl.v[i].v;
     }
     free(bl.v);
+}
 
+static int cmp_u32(const void* a, const void* b) {
+    uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+int or_add_batch(or_tree* t, const or_point* pts, uint32_t n) {
+    /* remolod_octree.cu:1181-1210 */
+    if (t->st.persistent_offset + t->cfg.safety_margin >= t->cfg.persistent_capacity) {
+        t->st.mem_capacity_reached = 1;
+        return 1;
+    }
+    t->st.mem_capacity_reached = 0;
+    const uint32_t batch_index = t->st.batchlet_index;
+    const uint32_t first_index = (uint32_t)t->st.num_points_processed;
+    t->spill_n = 0;
+
+    uint32_t* fresh_tag = (uint32_t*)calloc(t->cfg.max_nodes, sizeof(uint32_t));
+    if (!fresh_tag) abort();
+    /* nodes that exist count with countIteration = batchIndex (set in the previous batch) */
+    for (uint32_t i = 0; i < t->num_nodes; i++) fresh_tag[i] = batch_index;
+    expand(t, pts, n, batch_index, fresh_tag);
+    free(fresh_tag);
+    t->st.spilled_points += t->spill_n;
+
+    place_batch(t, pts, n, first_index);
     t->st.batchlet_index++;
     t->st.num_points_processed += n;
+    return 0;
+}
+
+/* Refinement's deepening (wiki/02_KernelPipeline.md:228-243, "local split
+ * and redistribute"). The leaves among nodes[0..n) holding at least
+ * min_points points (0 counts as 1) split as a batch's spilling nodes do
+ * (doSplitting, remolod_octree.cu:303-400): in increasing id, 8 consecutive
+ * ids each, refused by the pool guard once fewer than 8 remain (:318-321).
+ * That split is iteration 1 of an expand loop with no batch points: the
+ * later iterations count the spilled points into the new children and split
+ * any child over the limit (:402-462). The spilled points are then sampled
+ * into voxels and inserted as a batch's are. The memory check of a batch
+ * (:1181-1210) refuses the whole pass (returns 1). No batch is consumed:
+ * batchlet_index, num_points_processed and expand_iters stay. */
+int or_deepen(or_tree* t, const uint32_t* nodes, uint32_t n, uint32_t min_points, uint32_t* selected) {
+    if (selected) *selected = 0;
+    if (t->st.persistent_offset + t->cfg.safety_margin >= t->cfg.persistent_capacity) {
+        t->st.mem_capacity_reached = 1;
+        return 1;
+    }
+    t->st.mem_capacity_reached = 0;
+    const uint32_t minp = min_points ? min_points : 1u;
+    uint32_t* sel = (uint32_t*)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    if (!sel) abort();
+    uint32_t ns = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t ni = nodes[i];
+        if (ni < t->num_nodes && is_leaf(&t->nodes[ni]) && t->nodes[ni].level < OR_MAX_DEPTH &&
+            t->nodes[ni].num_points >= minp)
+            sel[ns++] = ni;
+    }
+    if (ns > OR_SPILLING_CAPACITY) {
+        t->st.overflow_flags |= OR_OVERFLOW_SPILLING;
+        ns = OR_SPILLING_CAPACITY;
+    }
+    if (selected) *selected = ns;
+    qsort(sel, ns, sizeof(uint32_t), cmp_u32);
+    const uint32_t batch_index = t->st.batchlet_index;
+    t->spill_n = 0;
+    uint32_t* fresh_tag = (uint32_t*)calloc(t->cfg.max_nodes, sizeof(uint32_t));
+    if (!fresh_tag) abort();
+    /* nodes that exist are not counted again in this pass */
+    for (uint32_t i = 0; i < t->num_nodes; i++) fresh_tag[i] = batch_index + 1u;
+    for (uint32_t k = 0; k < ns; k++) {
+        if (t->num_nodes + 8u > t->cfg.max_nodes) {
+            t->st.node_pool_overflow = 1;
+            continue;
+        }
+        const uint32_t base = t->num_nodes;
+        t->num_nodes += 8u;
+        split_node(t, sel[k], base);
+        t->st.nodes_split++;
+    }
+    t->st.num_nodes = t->num_nodes;
+    free(sel);
+    /* iterations 2.. of the loop: the seeded split was iteration 1 */
+    const uint32_t iters = t->cfg.max_expand_iters, done = t->st.expand_iters;
+    t->cfg.max_expand_iters = iters > 0u ? iters - 1u : 0u;
+    expand(t, NULL, 0, batch_index, fresh_tag);
+    t->cfg.max_expand_iters = iters;
+    t->st.expand_iters = done;
+    free(fresh_tag);
+    t->st.spilled_points += t->spill_n;
+    place_batch(t, NULL, 0, 0);
     return 0;
 }
 

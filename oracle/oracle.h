@@ -93,6 +93,11 @@ void or_reset(or_tree* t, const float box_min[3], const float box_max[3]);
 /* One batch through addBatch (remolod_octree.cu:940-1060). Returns 1 when the
  * memory check (remolod_octree.cu:1181-1210) refused the batch, else 0. */
 int or_add_batch(or_tree* t, const or_point* pts, uint32_t n);
+/* Refinement's deepening: the leaves among nodes[0..n) with at least
+ * min_points points split and their points redistributed, as a batch with no
+ * points whose spilling nodes they are. Returns 1 when the memory check
+ * refuses it; *selected: the leaves taken. */
+int or_deepen(or_tree* t, const uint32_t* nodes, uint32_t n, uint32_t min_points, uint32_t* selected);
 
 /* kernel_construct's batch loop over a ring (remolod_octree.cu:1169-1241),
  * without the wall-clock budget, then the stats sweep (:1271-1310). */

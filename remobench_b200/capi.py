@@ -71,6 +71,11 @@ class RefineResult(ctypes.Structure):
     _fields_ = [("nodes_filtered", u32), ("voxels_filtered", u32), ("points_visited", u64)]
 
 
+class DeepenResult(ctypes.Structure):
+    _fields_ = [("nodes_selected", u32), ("nodes_split", u32), ("nodes_refused", u32), ("stopped", u32),
+                ("points_moved", u64), ("voxels_made", u64)]
+
+
 class RenderResult(ctypes.Structure):
     _fields_ = [("draw_items", u32), ("drawlist_overflow", u32), ("draw_samples", u64), ("device_ms", f32),
                 ("pad", u32)]
@@ -144,6 +149,7 @@ SIGNATURES = {
     "rb_read_rollup": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_refine": (i32, [_vp, u32, u64]),
     "rb_refine_colors": (i32, [_vp, u32, ctypes.POINTER(RefineResult)]),
+    "rb_refine_deepen": (i32, [_vp, u32, u32, ctypes.POINTER(DeepenResult)]),
     "rb_read_features": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_mlp_init": (i32, [_vp, u64]),
     "rb_mlp_set_params": (i32, [_vp, _vp]),

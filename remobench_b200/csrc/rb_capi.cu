@@ -30,7 +30,7 @@ enum KernelId : int {
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
     K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_PASS, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE,
-    K_EXPAND_REST, K_WIREFRAME, K_REFINE_COLORS, K_ALLOC_VOXELS, K_FINISH_LEAVES, K_VOX_LIFT, K_VOX_SAMPLE_LEVELS, K_NUM
+    K_EXPAND_REST, K_WIREFRAME, K_REFINE_COLORS, K_ALLOC_VOXELS, K_FINISH_LEAVES, K_VOX_LIFT, K_VOX_SAMPLE_LEVELS, K_DEEPEN, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
@@ -41,7 +41,7 @@ static const char* const kKernelNames[K_NUM] = {
     "k_expand_cond", "k_zero_grids",
     // not a kernel: per-iteration expand passes run inside k_expand_rest
     "expand_pass", "k_deep_book", "k_deep_bin", "k_deep_split", "k_deep_move", "k_expand_rest",
-    "k_wireframe", "k_refine_colors", "k_alloc_voxels", "k_finish_leaves", "k_vox_lift", "k_vox_sample_levels"};
+    "k_wireframe", "k_refine_colors", "k_alloc_voxels", "k_finish_leaves", "k_vox_lift", "k_vox_sample_levels", "k_deepen"};
 
 struct Profiler {
     bool on = false;
@@ -221,19 +221,33 @@ __global__ void k_build_begin(Counters* c) {
 
 // One batch through addBatch's phases (remolod_octree.cu:940-1060). Returns
 // RB_OK with *stopped set when the memory check refused the batch.
+rb_status runBatchAfterCount(rb_ctx* c, const rb::Point* pts, uint32_t n, uint64_t work, bool* stopped, bool deepen);
+
 rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIndex, bool* stopped) {
     const Dev& d = c->d;
     cudaStream_t s = c->stream;
     *stopped = false;
     LAUNCH(c, K_BATCH_BEGIN, 1, rb::launchBatchBegin(d, s));
     LAUNCH(c, K_COUNT_FIRST, n, rb::launchCountFirst(d, pts, n, pointGrid(c, n), s));
+    return runBatchAfterCount(c, pts, n, n, stopped, false);
+}
+
+// The phases after the first count: the expand round, the per-iteration
+// passes, voxel sampling and insertion; a deepening pass (no batch points, its
+// spilling nodes taken from the Analysis queue) ends without counting a batch.
+// `work` sizes the grids of the point kernels.
+rb_status runBatchAfterCount(rb_ctx* c, const rb::Point* pts, uint32_t n, uint64_t work, bool* stopped,
+                             bool deepen) {
+    const Dev& d = c->d;
+    cudaStream_t s = c->stream;
+    *stopped = false;
     const int fixedGrid = c->numSMs * 4;
     // the same kernels as the batch graph, with k_expand_rest's loop on the
     // host; split and recount take their stamps from the device counters
     LAUNCH(c, K_DEEP_BOOK, 1, rb::launchDeepBook(d, s));
-    LAUNCH(c, K_DEEP_BIN, n, rb::launchDeepBin(d, pts, n, pointGrid(c, n), s));
+    LAUNCH(c, K_DEEP_BIN, n, rb::launchDeepBin(d, pts, n, pointGrid(c, work), s));
     LAUNCH(c, K_DEEP_SPLIT, 1, rb::launchDeepSplit(d, s));
-    LAUNCH(c, K_DEEP_MOVE, n, rb::launchDeepMove(d, pts, n, pointGrid(c, n), s));
+    LAUNCH(c, K_DEEP_MOVE, n, rb::launchDeepMove(d, pts, n, pointGrid(c, work), s));
     for (uint32_t pass = 0; pass < 64u; pass++) {
         rb_status st = readCounters(c);
         if (st != RB_OK) return st;
@@ -248,10 +262,9 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
         c->prof.launches[K_EXPAND_PASS] += 1;
         LAUNCH(c, K_SPLIT, c->hostCtr->numSpill, rb::launchSplit(d, 0u, s));
         LAUNCH(c, K_SPILL_COPY, 0, rb::launchSpillCopy(d, fixedGrid, s));
-        LAUNCH(c, K_RECOUNT, n, rb::launchRecount(d, pts, n, 0u, pointGrid(c, n), s));
+        LAUNCH(c, K_RECOUNT, n, rb::launchRecount(d, pts, n, 0u, pointGrid(c, work), s));
         LAUNCH(c, K_EXPAND_COND, 1, rb::launchExpandCond(d, s));
     }
-    const uint64_t work = n;
     LAUNCH(c, K_ZERO_GRIDS, 0, rb::launchZeroGrids(d, fixedGrid, s));
     LAUNCH(c, K_FINISH_LEAVES, n, rb::launchFinishLeaves(d, pts, n, pointGrid(c, work), s));
     LAUNCH(c, K_VOX_SAMPLE, n, rb::launchVoxSample(d, pts, n, pointGrid(c, work), s));
@@ -263,7 +276,8 @@ rb_status runBatch(rb_ctx* c, const rb::Point* pts, uint32_t n, uint32_t batchIn
     LAUNCH(c, K_VOX_STORE, 0, rb::launchVoxStore(d, fixedGrid, s));
     LAUNCH(c, K_ALLOC_POINTS, 0, rb::launchAllocPoints(d, fixedGrid, s));
     LAUNCH(c, K_INSERT, n, rb::launchInsert(d, pts, n, pointGrid(c, work), s));
-    LAUNCH(c, K_BATCH_END, 1, rb::launchBatchEnd(d, n, s));
+    if (deepen) LAUNCH(c, K_DEEPEN, 1, rb::launchDeepenEnd(d, s));
+    else LAUNCH(c, K_BATCH_END, 1, rb::launchBatchEnd(d, n, s));
     RB_CUDA(c, cudaGetLastError());
     return RB_OK;
 }
@@ -1426,6 +1440,43 @@ rb_status rb_refine_colors(rb_ctx* c, uint32_t budget, rb_refine_result* out) {
         out->nodes_filtered = c->hostRefine->nodes;
         out->voxels_filtered = c->hostRefine->voxels;
         out->points_visited = c->hostRefine->points;
+    }
+    return RB_OK;
+}
+
+rb_status rb_refine_deepen(rb_ctx* c, uint32_t budget, uint32_t min_points, rb_deepen_result* out) {
+    if (!c) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
+    if (!c->analyzed) return fail(c, RB_ERR_STATE, "refine before rb_analyze");
+    if (out) std::memset(out, 0, sizeof(*out));
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    const uint64_t splitBefore = c->hostCtr->nodesSplit;
+    const uint32_t nodesBefore = c->hostCtr->numNodes;
+    const uint32_t qlen = c->hostActr->queueLength;
+    LAUNCH(c, K_DEEPEN, 1, rb::launchDeepenBegin(c->d, c->aqueue, qlen, budget, min_points, c->stream));
+    bool stopped = false;
+    // no batch points: every phase reads the spill list only
+    st = runBatchAfterCount(c, c->d.spillPts, 0u, (uint64_t)c->numSMs * 8u * 256u, &stopped, true);
+    if (st != RB_OK) return st;
+    if ((st = readCounters(c)) != RB_OK) return st;
+    const rb::Counters& k = *c->hostCtr;
+    // the queue names nodes by their role before the pass
+    c->analyzed = false;
+    if (out) {
+        out->stopped = k.batchStop ? 1u : 0u;
+        out->nodes_selected = k.batchStop ? 0u : k.deepenSelected;
+        out->nodes_split = (uint32_t)(k.nodesSplit - splitBefore);
+        const uint32_t room = c->cfg.max_nodes > nodesBefore ? (c->cfg.max_nodes - nodesBefore) / 8u : 0u;
+        out->nodes_refused = out->nodes_selected > room ? out->nodes_selected - room : 0u;
+        out->points_moved = k.batchStop ? 0u : k.numSpilled;
+        const uint64_t made = (uint64_t)k.numNew + k.numLift;
+        out->voxels_made = k.batchStop ? 0u : (made < c->d.newCap ? made : c->d.newCap);
+    }
+    if (!k.batchStop && c->cfg.accumulate && c->cfg.pipeline == RB_PIPELINE_REMOLOD) {
+        if ((st = accumulate(c, k.batchletIndex)) != RB_OK) return st;
+        RB_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     return RB_OK;
 }

@@ -57,6 +57,7 @@ struct Counters {
     uint32_t numNew;              // new voxel cells this batch
     uint32_t numLift;             // new voxel cells k_vox_lift listed after numNew
     uint32_t levelMode;           // this batch samples voxels level by level (gridsPartial at its start)
+    uint32_t deepenSelected;      // leaves a deepening pass took from the queue
     uint32_t spillChunkTotal;     // copy work items of the last split
     uint32_t loopMore;            // the last loop test's answer: another expand pass
     // flags and diagnostics (sticky until reset)

@@ -196,6 +196,8 @@ __device__ __forceinline__ uint32_t blockReserve(BlockSlots& b, uint32_t* counte
     return key == kNone ? kNone : (s != kNone ? b.base[s] : 0u) + off + rank;
 }
 
+__device__ __forceinline__ void resetBatchCounters(Counters* c);
+
 __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     Counters* c = d.ctr;
     uint32_t reason = 0;
@@ -229,6 +231,11 @@ __global__ void k_batch_begin(Dev d, uint32_t fromRing) {
     else if (reason == 0) c->memCapacityReached = 0u;
     c->batchStop = reason ? 1u : 0u;
     c->stopReason = reason;
+    resetBatchCounters(c);
+}
+
+// The per-batch state every batch (and a deepening pass) starts from.
+__device__ __forceinline__ void resetBatchCounters(Counters* c) {
     c->numSpill = 0;
     c->numSpilled = 0;
     c->numNew = 0;
@@ -2329,6 +2336,68 @@ __global__ void __launch_bounds__(256) k_vox_store(Dev d) {
     }
 }
 
+// Refinement's deepening (wiki/02_KernelPipeline.md:228-243: "local split and
+// redistribute", listed by the reference and not built there), begun like a
+// batch with no points: the memory check of a batch (remolod_octree.cu:1181-1210),
+// the per-batch state, then the leaves among the first `budget` queue entries
+// above the deepest level with at least minPoints stored points become this
+// pass's spilling nodes, in queue order. The batch kernels that follow (the expand round from
+// k_deep_book, or the per-iteration passes) split them as doSplitting would:
+// 8 consecutive ids each in increasing id, the pool guard refusing once fewer
+// than 8 remain (:318-321), their stored points to the spill list and their
+// chunks to the queue; voxel sampling gives each its voxels; insertion puts the
+// points into the children. One block.
+__global__ void __launch_bounds__(1024) k_deepen_begin(Dev d, const uint32_t* queue, uint32_t queueLen,
+                                                         uint32_t budget, uint32_t minPoints) {
+    __shared__ uint32_t s_warp[32];
+    Counters* c = d.ctr;
+    if (threadIdx.x == 0) {
+        const bool full = c->refOffset + d.safetyMargin >= d.persistentCapacity;
+        c->memCapacityReached = full ? 1u : 0u;
+        c->batchStop = full ? 1u : 0u;
+        c->stopReason = full ? kStopMemory : 0u;
+        resetBatchCounters(c);
+        c->curN = 0;
+        c->deepenSelected = 0;
+    }
+    __syncthreads();
+    if (c->batchStop) return;
+    const uint32_t k = budget < queueLen ? budget : queueLen;
+    const uint32_t minPts = minPoints > 0u ? minPoints : 1u;
+    uint32_t count = 0;
+    for (uint32_t b = 0; b < k; b += blockDim.x) {
+        const uint32_t i = b + threadIdx.x;
+        uint32_t node = kNone, take = 0;
+        if (i < k) {
+            node = queue[i];
+            take = node < c->numNodes && isLeaf(d, node) && d.level[node] < (uint32_t)kMaxDepth &&
+                           d.numPoints[node] >= minPts
+                       ? 1u
+                       : 0u;
+        }
+        uint32_t tot;
+        const uint32_t pre = blockExclusiveScan(take, &tot, s_warp);
+        if (take && count + pre < d.spillingCap) d.spillNodes[count + pre] = node;
+        count += tot;
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t sel = count < d.spillingCap ? count : d.spillingCap;
+        if (count > d.spillingCap) atomicOr(&c->overflowFlags, (uint32_t)kOvfSpilling);
+        c->numSpill = sel;
+        c->deepenSelected = sel;
+    }
+}
+
+// The end of a deepening pass: a batch's bookkeeping without a batch (the
+// batch index and the points processed stay).
+__global__ void k_deepen_end(Dev d) {
+    Counters* c = d.ctr;
+    if (c->batchStop) return;
+    if (c->numAllocatedChunks > c->chunkPoolSize) c->chunkPoolSize = c->numAllocatedChunks;
+    c->spilledPointsTotal += c->numSpilled;
+    if (c->iter > d.maxExpandIters) c->arrivalMode = 1u;
+}
+
 // n == kNone: the batch at the device cursor.
 __global__ void k_batch_end(Dev d, uint32_t n) {
     Counters* c = d.ctr;
@@ -2410,6 +2479,11 @@ __global__ void k_reset_root(Dev d) {
 // ------------------------------------------------------------------ launches
 
 void launchBatchBegin(const Dev& d, cudaStream_t s) { k_batch_begin<<<1, 1, 0, s>>>(d, 0u); }
+void launchDeepenBegin(const Dev& d, const uint32_t* queue, uint32_t queueLen, uint32_t budget, uint32_t minPoints,
+                       cudaStream_t s) {
+    k_deepen_begin<<<1, 1024, 0, s>>>(d, queue, queueLen, budget, minPoints);
+}
+void launchDeepenEnd(const Dev& d, cudaStream_t s) { k_deepen_end<<<1, 1, 0, s>>>(d); }
 void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_count_first<<<grid, 256, 0, s>>>(d, pts, n);
 }

@@ -259,6 +259,13 @@ class Context:
         self._ok(capi.lib().rb_refine_colors(self.h, int(budget), ctypes.byref(r)))
         return r
 
+    def refine_deepen(self, budget, min_points=0):
+        """Deepening of the queued leaves among the first `budget` queue entries
+        (rb_refine_deepen): split and their points redistributed."""
+        r = capi.DeepenResult()
+        self._ok(capi.lib().rb_refine_deepen(self.h, int(budget), int(min_points), ctypes.byref(r)))
+        return r
+
     def set_stream(self, stream_handle):
         self._ok(capi.lib().rb_set_stream(self.h, ctypes.c_void_p(int(stream_handle))))
 

@@ -250,3 +250,69 @@ def test_colour_filtering_known_answer():
     assert (c & 255, (c >> 8) & 255, (c >> 16) & 255, c >> 24) == (mean[0], mean[1], mean[2], 200)
     # a capacity below the node's voxels filters nothing
     assert t.refine_colors([0], capacity=0) == (0, 0)
+
+
+def test_deepen_known_answer():
+    # Refinement's deepening: five points split the root (limit 4); child 1
+    # (octant 0) keeps three. Deepening it splits it as doSplitting would
+    # (remolod_octree.cu:303-400): ids 9..16, its points one level down by bit
+    # 18 of the 20-bit coordinate, and a grid sampled at level 1, whose cell
+    # is the 28-bit coordinate >> 20 (0.1 -> 25, 0.3 -> 76).
+    t = unit_tree(max_points_per_node=4)
+    cloud = pts([(0.1, 0.1, 0.1, 11), (0.3, 0.1, 0.1, 12), (0.1, 0.1, 0.3, 13),
+                 (0.9, 0.9, 0.9, 14), (0.6, 0.2, 0.9, 15)])
+    assert t.add_batch(cloud) == 0
+    t.sweep()
+    c1 = t.node(1)
+    assert c1.is_leaf and c1.num_points == 3 and (c1.level, c1.X, c1.Y, c1.Z) == (1, 0, 0, 0)
+    before = t.stats()
+    refused, taken = t.deepen([1, 4], min_points=2)  # node 4 holds fewer than 2 points
+    assert not refused and taken == 1
+    t.sweep()
+    s = t.stats()
+    assert s.num_nodes == 17 and s.nodes_split == before.nodes_split + 1
+    assert (s.batchlet_index, s.num_points_processed) == (before.batchlet_index, before.num_points_processed)
+    c1 = t.node(1)
+    assert not c1.is_leaf and list(c1.child) == list(range(9, 17)) and c1.num_points == 0
+    # octants at level 1: (0.1,.1,.1) -> 0, (0.3,.1,.1) -> 4, (0.1,.1,.3) -> 1
+    got = {k: list(t.leaf_points(9 + k)[1]) for k in range(8) if t.node(9 + k).num_points}
+    assert got == {0: [0], 1: [2], 4: [1]}
+    v = np.sort(t.node_voxels(1), order=["x", "y", "z"])
+    cells = [(25, 25, 25, 11), (25, 25, 76, 13), (76, 25, 25, 12)]
+    assert len(v) == 3
+    for row, (cx, cy, cz, col) in zip(v, sorted(cells)):
+        assert row["x"] == np.float32(0.5 * (cx + 0.5) / 128)
+        assert row["y"] == np.float32(0.5 * (cy + 0.5) / 128)
+        assert row["z"] == np.float32(0.5 * (cz + 0.5) / 128)
+        assert row["color"] == col
+
+
+def test_deepen_keeps_every_point_and_samples_the_deepened_nodes(c1_cloud):
+    cfg, cloud, bmin, bmax = c1_cloud
+    t = ob.Tree(num_threads=4)
+    t.reset(bmin, bmax)
+    bs = cfg.batch_size
+    for b in range(6):
+        assert t.add_batch(cloud[b * bs:(b + 1) * bs]) == 0
+    nodes = t.node_table()
+    leaves = np.nonzero(nodes["is_leaf"] & (nodes["num_points"] > 0))[0]
+    pick = leaves[np.argsort(-nodes["num_points"][leaves], kind="stable")][:12]
+    before = t.stats()
+    refused, taken = t.deepen(pick)
+    assert not refused and taken == len(pick)
+    for b in range(6, 8):
+        assert t.add_batch(cloud[b * bs:(b + 1) * bs]) == 0
+    t.sweep()
+    s = t.stats()
+    assert s.num_points == len(cloud) and s.dropped_points == 0 and s.overflow_flags == 0
+    assert s.nodes_split >= before.nodes_split + len(pick)
+    g = t.accumulate(8)
+    assert g.sum_leaf_counts == len(cloud) and g.inner_with_sums == 0
+    seen = np.zeros(len(cloud), dtype=np.int32)
+    after = t.node_table()
+    for i in np.nonzero(after["is_leaf"])[0]:
+        seen[t.leaf_points(int(i))[1]] += 1
+    assert np.all(seen == 1)
+    for i in pick:
+        assert after["is_leaf"][i] == 0 and after["num_voxels"][i] > 0
+        assert after["num_voxels"][i] == int(sum(bin(int(w)).count("1") for w in t.node_grid(int(i))))

@@ -414,6 +414,26 @@ typedef struct rb_deepen_result {
 } rb_deepen_result;
 rb_status rb_refine_deepen(struct rb_ctx* ctx, uint32_t budget, uint32_t min_points, rb_deepen_result* out);
 
+/* Refinement's collapsing (wiki/02_KernelPipeline.md:228-243, "merge a node
+ * back up"; the reference lists it, unbuilt, since it needs a grid pool,
+ * CLAUDE.md:185-187). Among the `count` node ids at nodes (host memory, at
+ * most 4096; duplicates ignored), every node below the root whose eight
+ * children are all leaves holding at most max_points points together (0: the
+ * split limit) becomes a leaf again with all their points. Its chunks are
+ * allocated first, then the children's chunks return to the queue; the
+ * children stay as empty leaves nothing points to (node ids are not reused);
+ * the node drops its voxels and returns its grid to a pool that later splits
+ * take grids from before the arena. No batch is consumed; Accumulate runs
+ * after it (remolod); an Analysis queue is stale afterwards. */
+typedef struct rb_collapse_result {
+    uint32_t nodes_collapsed;
+    uint32_t grids_returned;
+    uint64_t points_moved;     /* points now held by the merged leaves */
+    uint64_t voxels_dropped;   /* voxels the merged nodes held */
+} rb_collapse_result;
+rb_status rb_refine_collapse(struct rb_ctx* ctx, const uint32_t* nodes, uint32_t count, uint32_t max_points,
+                             rb_collapse_result* out);
+
 /* The learned scorer (no reference counterpart: plans/04_NeuralPass.md is
  * empty): a 16 -> 64 -> 64 -> 2 MLP, GELU, BF16 weights and activations, FP32
  * accumulation, trained on the GPU with these entry points. Inputs are the 16

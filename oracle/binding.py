@@ -196,6 +196,7 @@ def lib():
         L.or_features.argtypes = [vp, u32, u32, vp]
         L.or_refine_colors.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u64)]
         L.or_deepen.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u32)]
+        L.or_collapse.argtypes = [vp, vp, u32, u32, ctypes.POINTER(u32), ctypes.POINTER(u64), ctypes.POINTER(u64)]
         L.or_deepen.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -318,6 +319,14 @@ class Tree:
         m = ctypes.c_uint32()
         rc = lib().or_deepen(self.h, _ptr(arr), len(arr), min_points, ctypes.byref(m))
         return rc != 0, m.value
+
+    def collapse(self, nodes, max_points=0):
+        """Refinement's collapsing of the listed nodes; (collapsed, points moved,
+        voxels dropped)."""
+        arr = np.ascontiguousarray(nodes, dtype=np.uint32)
+        m, p, v = ctypes.c_uint32(), ctypes.c_uint64(), ctypes.c_uint64()
+        lib().or_collapse(self.h, _ptr(arr), len(arr), max_points, ctypes.byref(m), ctypes.byref(p), ctypes.byref(v))
+        return m.value, p.value, v.value
 
     def accumulate(self, batch_index):
         g = AccumGlobals()

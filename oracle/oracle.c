@@ -58,6 +58,9 @@ struct or_tree {
     uint32_t num_nodes;
     uint32_t** grids;
     uint32_t num_grids, grids_cap;
+    /* grids collapsed nodes returned; splits take them before new ones */
+    int32_t* grid_pool;
+    uint32_t grid_pool_n, grid_pool_cap;
     float box_min[3], box_max[3];
     float octree_size;
     or_stats st;
@@ -134,6 +137,11 @@ static uint64_t ref_alloc_size(uint64_t size) { return 16ull * ((size + 16ull) /
 static uint32_t ceil_div(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
 
 static int32_t new_grid(or_tree* t) {
+    if (t->grid_pool_n > 0) {
+        const int32_t g = t->grid_pool[--t->grid_pool_n];
+        memset(t->grids[g], 0, OR_GRID_WORDS * sizeof(uint32_t));
+        return g;
+    }
     if (t->num_grids == t->grids_cap) {
         uint32_t cap = t->grids_cap ? 2u * t->grids_cap : 64u;
         uint32_t** g = (uint32_t**)realloc(t->grids, cap * sizeof(uint32_t*));
@@ -191,6 +199,7 @@ static void release_all(or_tree* t) {
     for (uint32_t i = 0; i < t->num_nodes; i++) node_free_storage(&t->nodes[i]);
     for (uint32_t g = 0; g < t->num_grids; g++) free(t->grids[g]);
     t->num_grids = 0;
+    t->grid_pool_n = 0;
     t->num_nodes = 0;
 }
 
@@ -198,6 +207,7 @@ void or_destroy(or_tree* t) {
     if (!t) return;
     release_all(t);
     free(t->grids);
+    free(t->grid_pool);
     free(t->nodes);
     free(t->spill);
     free(t);
@@ -689,6 +699,125 @@ int or_deepen(or_tree* t, const uint32_t* nodes, uint32_t n, uint32_t min_points
     return 0;
 }
 
+/* Refinement's collapsing ("merge a node back up",
+ * wiki/02_KernelPipeline.md:228-243; it needs a grid pool, CLAUDE.md:185-187).
+ * Each node among nodes[0..n) (duplicates ignored) below the root whose
+ * eight children are all leaves holding at most max_points points together
+ * (0: the split limit) becomes a leaf with their points, in child order. Its
+ * chunks are taken first, as allocatePointChunks takes them (:742-792):
+ * recycled, then new ones charged to the store; then the children's chunks
+ * return to the queue and the children are left empty with nothing pointing
+ * to them. The node drops its voxels and returns its grid to the pool; its
+ * exact sums restart, so the next Accumulate folds all its points. */
+int or_collapse(or_tree* t, const uint32_t* nodes, uint32_t n, uint32_t max_points, uint32_t* collapsed,
+                uint64_t* points, uint64_t* voxels) {
+    const uint32_t ppc = t->cfg.points_per_chunk;
+    const uint32_t maxp = max_points ? max_points : t->cfg.max_points_per_node;
+    uint32_t* ids = (uint32_t*)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    uint32_t* rec = (uint32_t*)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    if (!ids || !rec) abort();
+    memcpy(ids, nodes, (size_t)n * sizeof(uint32_t));
+    qsort(ids, n, sizeof(uint32_t), cmp_u32);
+    uint32_t nr = 0;
+    uint64_t moved = 0, dropped = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t ni = ids[i];
+        if ((i > 0 && ids[i - 1] == ni) || ni >= t->num_nodes) continue;
+        const onode* nd = &t->nodes[ni];
+        if (nd->level == 0 || is_leaf(nd)) continue;
+        uint64_t total = 0;
+        int ok = 1;
+        for (int q = 0; q < 8 && ok; q++) {
+            const int32_t ch = nd->child[q];
+            if (ch < 0 || !is_leaf(&t->nodes[ch])) ok = 0;
+            else {
+                const onode* c = &t->nodes[ch];
+                const uint32_t cap = c->num_point_chunks * ppc;
+                total += c->num_points < cap ? c->num_points : cap;
+            }
+        }
+        if (ok && total <= maxp) rec[nr++] = ni;
+    }
+    /* the merged leaves' chunks first */
+    const uint64_t pool_before = t->st.chunk_pool_size;
+    for (uint32_t k = 0; k < nr; k++) {
+        onode* nd = &t->nodes[rec[k]];
+        uint32_t total = 0;
+        for (int q = 0; q < 8; q++) {
+            const onode* c = &t->nodes[nd->child[q]];
+            const uint32_t cap = c->num_point_chunks * ppc;
+            total += c->num_points < cap ? c->num_points : cap;
+        }
+        const uint32_t req = ceil_div(total, ppc);
+        for (uint32_t e = 0; e < req; e++) {
+            const uint64_t ci = t->st.num_allocated_chunks++;
+            if (ci >= pool_before) t->st.persistent_offset += ref_alloc_size(OR_CHUNK_BYTES);
+        }
+        ensure_pts_cap(nd, req * ppc > 0 ? req * ppc : 1);
+        uint32_t at = 0;
+        for (int q = 0; q < 8; q++) {
+            const onode* c = &t->nodes[nd->child[q]];
+            const uint32_t cap = c->num_point_chunks * ppc;
+            const uint32_t np = c->num_points < cap ? c->num_points : cap;
+            if (np) {
+                memcpy(nd->pts + at, c->pts, (size_t)np * sizeof(or_point));
+                memcpy(nd->idx + at, c->idx, (size_t)np * sizeof(uint32_t));
+            }
+            at += np;
+        }
+        nd->num_point_chunks = req;
+        nd->num_points = total;
+        nd->counter = total;
+        moved += total;
+    }
+    if (t->st.num_allocated_chunks > t->st.chunk_pool_size) t->st.chunk_pool_size = t->st.num_allocated_chunks;
+    /* then the children's chunks back to the queue, the voxels and the grid */
+    for (uint32_t k = 0; k < nr; k++) {
+        onode* nd = &t->nodes[rec[k]];
+        for (int q = 0; q < 8; q++) {
+            onode* c = &t->nodes[nd->child[q]];
+            t->st.num_allocated_chunks -= c->num_point_chunks;
+            free(c->pts);
+            free(c->idx);
+            c->pts = NULL;
+            c->idx = NULL;
+            c->pts_cap = 0;
+            c->num_points = 0;
+            c->counter = 0;
+            c->num_point_chunks = 0;
+            memset(&c->ai, 0, sizeof(c->ai));
+            memset(&c->af, 0, sizeof(c->af));
+            nd->child[q] = -1;
+        }
+        dropped += nd->num_voxels;
+        free(nd->vox);
+        nd->vox = NULL;
+        nd->vox_cap = 0;
+        nd->num_voxels = 0;
+        nd->num_voxels_stored = 0;
+        nd->num_voxel_chunks = 0;
+        if (nd->grid >= 0) {
+            if (t->grid_pool_n == t->grid_pool_cap) {
+                uint32_t cap = t->grid_pool_cap ? 2u * t->grid_pool_cap : 64u;
+                int32_t* g = (int32_t*)realloc(t->grid_pool, cap * sizeof(int32_t));
+                if (!g) abort();
+                t->grid_pool = g;
+                t->grid_pool_cap = cap;
+            }
+            t->grid_pool[t->grid_pool_n++] = nd->grid;
+            nd->grid = -1;
+        }
+        memset(&nd->ai, 0, sizeof(nd->ai));
+        memset(&nd->af, 0, sizeof(nd->af));
+    }
+    free(ids);
+    free(rec);
+    if (collapsed) *collapsed = nr;
+    if (points) *points = moved;
+    if (voxels) *voxels = dropped;
+    return 0;
+}
+
 /* stats sweep (remolod_octree.cu:1271-1310) */
 void or_sweep(or_tree* t) {
     or_stats* s = &t->st;
@@ -714,7 +843,7 @@ void or_sweep(or_tree* t) {
         }
     }
     s->num_nodes = t->num_nodes;
-    s->num_grids = t->num_grids;
+    s->num_grids = t->num_grids - t->grid_pool_n;
 }
 
 uint32_t or_build(or_tree* t, const or_point* ring, const uint32_t* batch_sizes,

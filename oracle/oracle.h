@@ -98,6 +98,11 @@ int or_add_batch(or_tree* t, const or_point* pts, uint32_t n);
  * points whose spilling nodes they are. Returns 1 when the memory check
  * refuses it; *selected: the leaves taken. */
 int or_deepen(or_tree* t, const uint32_t* nodes, uint32_t n, uint32_t min_points, uint32_t* selected);
+/* Refinement's collapsing: each listed node whose children are all leaves
+ * holding at most max_points points (0: the split limit) becomes a leaf with
+ * their points; its grid goes to a pool later splits take from. */
+int or_collapse(or_tree* t, const uint32_t* nodes, uint32_t n, uint32_t max_points, uint32_t* collapsed,
+                uint64_t* points, uint64_t* voxels);
 
 /* kernel_construct's batch loop over a ring (remolod_octree.cu:1169-1241),
  * without the wall-clock budget, then the stats sweep (:1271-1310). */

@@ -76,6 +76,10 @@ class DeepenResult(ctypes.Structure):
                 ("points_moved", u64), ("voxels_made", u64)]
 
 
+class CollapseResult(ctypes.Structure):
+    _fields_ = [("nodes_collapsed", u32), ("grids_returned", u32), ("points_moved", u64), ("voxels_dropped", u64)]
+
+
 class RenderResult(ctypes.Structure):
     _fields_ = [("draw_items", u32), ("drawlist_overflow", u32), ("draw_samples", u64), ("device_ms", f32),
                 ("pad", u32)]
@@ -150,6 +154,7 @@ SIGNATURES = {
     "rb_refine": (i32, [_vp, u32, u64]),
     "rb_refine_colors": (i32, [_vp, u32, ctypes.POINTER(RefineResult)]),
     "rb_refine_deepen": (i32, [_vp, u32, u32, ctypes.POINTER(DeepenResult)]),
+    "rb_refine_collapse": (i32, [_vp, _vp, u32, u32, ctypes.POINTER(CollapseResult)]),
     "rb_read_features": (i32, [_vp, _vp, u32, ctypes.POINTER(u32)]),
     "rb_mlp_init": (i32, [_vp, u64]),
     "rb_mlp_set_params": (i32, [_vp, _vp]),

@@ -30,7 +30,7 @@ enum KernelId : int {
     K_SWEEP, K_RESET_ROOT, K_FB_CLEAR, K_NODE_FLAGS, K_FRONTIER, K_RASTER, K_RASTER_FLAT, K_EDL,
     K_RESOLVE, K_ROLL, K_ANALYZE, K_QUEUE, K_REFINE, K_SCORE, K_MLP_PREDICT, K_MLP_GRAD, K_MLP_ADAM,
     K_EXPAND_COND, K_ZERO_GRIDS, K_EXPAND_PASS, K_DEEP_BOOK, K_DEEP_BIN, K_DEEP_SPLIT, K_DEEP_MOVE,
-    K_EXPAND_REST, K_WIREFRAME, K_REFINE_COLORS, K_ALLOC_VOXELS, K_FINISH_LEAVES, K_VOX_LIFT, K_VOX_SAMPLE_LEVELS, K_DEEPEN, K_NUM
+    K_EXPAND_REST, K_WIREFRAME, K_REFINE_COLORS, K_ALLOC_VOXELS, K_FINISH_LEAVES, K_VOX_LIFT, K_VOX_SAMPLE_LEVELS, K_DEEPEN, K_COLLAPSE, K_NUM
 };
 static const char* const kKernelNames[K_NUM] = {
     "k_build_begin", "k_batch_begin", "k_count_first", "k_split", "k_spill_copy", "k_recount",
@@ -41,7 +41,7 @@ static const char* const kKernelNames[K_NUM] = {
     "k_expand_cond", "k_zero_grids",
     // not a kernel: per-iteration expand passes run inside k_expand_rest
     "expand_pass", "k_deep_book", "k_deep_bin", "k_deep_split", "k_deep_move", "k_expand_rest",
-    "k_wireframe", "k_refine_colors", "k_alloc_voxels", "k_finish_leaves", "k_vox_lift", "k_vox_sample_levels", "k_deepen"};
+    "k_wireframe", "k_refine_colors", "k_alloc_voxels", "k_finish_leaves", "k_vox_lift", "k_vox_sample_levels", "k_deepen", "k_collapse"};
 
 struct Profiler {
     bool on = false;
@@ -576,6 +576,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.splitIter, N, "split stamps");
     ALLOC(d.anc, (uint64_t)N * rb::kMaxDepth, "ancestor table");
     ALLOC(d.parent, N, "parent table");
+    ALLOC(d.gridPool, N, "grid pool");
     ALLOC(d.dirtyStamp, N, "dirty stamps");
     ALLOC(d.accum, N, "accumulators");
     ALLOC(d.dirtyList, N, "dirty list");
@@ -1475,6 +1476,39 @@ rb_status rb_refine_deepen(rb_ctx* c, uint32_t budget, uint32_t min_points, rb_d
         out->voxels_made = k.batchStop ? 0u : (made < c->d.newCap ? made : c->d.newCap);
     }
     if (!k.batchStop && c->cfg.accumulate && c->cfg.pipeline == RB_PIPELINE_REMOLOD) {
+        if ((st = accumulate(c, k.batchletIndex)) != RB_OK) return st;
+        RB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return RB_OK;
+}
+
+rb_status rb_refine_collapse(rb_ctx* c, const uint32_t* nodes, uint32_t count, uint32_t max_points,
+                             rb_collapse_result* out) {
+    if (!c || (count && !nodes)) return RB_ERR_INVALID_ARG;
+    if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
+    if (count > 4096u || count > c->d.spillingCap)
+        return fail(c, RB_ERR_CAPACITY, "collapse takes at most 4096 candidate nodes per call");
+    if (out) std::memset(out, 0, sizeof(*out));
+    if (count == 0) return RB_OK;
+    RB_CUDA(c, cudaSetDevice(c->device));
+    rb_status st = readCounters(c);
+    if (st != RB_OK) return st;
+    const uint32_t poolBefore = c->hostCtr->gridPoolSize;
+    RB_CUDA(c, cudaMemsetAsync(&c->d.ctr->collapsePoints, 0, 2 * sizeof(unsigned long long), c->stream));
+    RB_CUDA(c, cudaMemcpyAsync(c->d.spillNodes, nodes, (size_t)count * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                               c->stream));
+    LAUNCH(c, K_COLLAPSE, count, rb::launchCollapse(c->d, count, max_points, c->numSMs * 4, c->stream));
+    RB_CUDA(c, cudaGetLastError());
+    if ((st = readCounters(c)) != RB_OK) return st;
+    const rb::Counters& k = *c->hostCtr;
+    c->analyzed = false;
+    if (out) {
+        out->nodes_collapsed = k.collapseSelected;
+        out->grids_returned = k.gridPoolSize - poolBefore;
+        out->points_moved = k.collapsePoints;
+        out->voxels_dropped = k.collapseVoxels;
+    }
+    if (k.collapseSelected && c->cfg.accumulate && c->cfg.pipeline == RB_PIPELINE_REMOLOD) {
         if ((st = accumulate(c, k.batchletIndex)) != RB_OK) return st;
         RB_CUDA(c, cudaStreamSynchronize(c->stream));
     }

@@ -53,6 +53,7 @@ void launchVoxSampleLevels(const Dev& d, const Point* pts, uint32_t n, int grid,
 void launchDeepenBegin(const Dev& d, const uint32_t* queue, uint32_t queueLen, uint32_t budget, uint32_t minPoints,
                        cudaStream_t s);
 void launchDeepenEnd(const Dev& d, cudaStream_t s);
+void launchCollapse(const Dev& d, uint32_t count, uint32_t maxPoints, int grid, cudaStream_t s);
 void launchVoxCommit(const Dev& d, int grid, cudaStream_t s);
 void launchFinishLeaves(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s);
 void launchAllocPoints(const Dev& d, int grid, cudaStream_t s);

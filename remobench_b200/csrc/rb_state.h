@@ -58,6 +58,12 @@ struct Counters {
     uint32_t numLift;             // new voxel cells k_vox_lift listed after numNew
     uint32_t levelMode;           // this batch samples voxels level by level (gridsPartial at its start)
     uint32_t deepenSelected;      // leaves a deepening pass took from the queue
+    uint32_t collapseSelected;    // nodes a collapsing pass merges
+    uint32_t collapseItems;       // their children's point chunks (copy and release work items)
+    unsigned long long collapsePoints;  // points the pass moved into the merged leaves
+    unsigned long long collapseVoxels;  // voxels the merged nodes dropped
+    uint32_t gridPoolSize;        // grids collapsed nodes returned (Dev::gridPool), taken again by splits
+    uint32_t gridPoolTaken;       // pool grids taken in this batch (settled at its end)
     uint32_t spillChunkTotal;     // copy work items of the last split
     uint32_t loopMore;            // the last loop test's answer: another expand pass
     // flags and diagnostics (sticky until reset)
@@ -204,6 +210,7 @@ struct Dev {
     // grid a point of n must test, with no pointer chase.
     uint2* anc;              // [maxNodes * kMaxDepth]
     uint2* parent;           // [maxNodes] (id, grid) of the parent: row n of anc at level(n) - 1
+    uint32_t* gridPool;      // [maxNodes] grids returned by collapsed nodes
     uint32_t* dirtyStamp;
     AccumI* accum;
     // storage: one arena in 16-byte units holding grids (256 KB), point chunks

@@ -504,6 +504,25 @@ __device__ __forceinline__ uint32_t warpSortAscending(uint32_t v) {
     return v;
 }
 
+// A grid for a node that splits: one a collapsed node returned (already
+// charged to the store), else a new one from the arena, charged as the
+// reference's allocator charges it. Pool grids are zeroed with the others.
+__device__ __forceinline__ uint32_t takeGrid(const Dev& d, Counters* c) {
+    atomicAdd(&c->numGrids, 1u);
+    const uint32_t k = atomicAdd(&c->gridPoolTaken, 1u);
+    const uint32_t pool = c->gridPoolSize;
+    if (k < pool) return d.gridPool[pool - 1u - k];
+    atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset), (unsigned long long)refAllocSize(kGridBytes));
+    return arenaAlloc(d, kGridUnits);
+}
+
+// The pool after a batch: the grids its splits took are gone from it.
+__device__ __forceinline__ void settleGridPool(Counters* c) {
+    const uint32_t t = c->gridPoolTaken < c->gridPoolSize ? c->gridPoolTaken : c->gridPoolSize;
+    c->gridPoolSize -= t;
+    c->gridPoolTaken = 0;
+}
+
 // The bookkeeping of the k-th split node of a pass (remolod_octree.cu:303-400):
 // its grid, its split stamp, its record for the spill copy (spill slots and
 // copy items from the given prefixes), its chunks' queue positions, the grid
@@ -513,10 +532,8 @@ __device__ __forceinline__ void splitBook(const Dev& d, Counters* c, uint32_t k,
                                           SplitInfo* s_info) {
     uint32_t g = d.grid[node];
     if (g == kNone) {
-        g = arenaAlloc(d, kGridUnits);
+        g = takeGrid(d, c);
         d.grid[node] = g;
-        atomicAdd(&c->numGrids, 1u);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset), (unsigned long long)refAllocSize(kGridBytes));
     }
     d.splitIter[node] = stamp;
     SplitRec r;
@@ -738,11 +755,8 @@ __device__ __forceinline__ void splitBody(const Dev& d, uint32_t stamp, uint32_t
             const uint32_t j = s_run2 + pre;
             if (f && j < room2) {
                 const uint32_t node = nn + t;
-                uint32_t g = arenaAlloc(d, kGridUnits);
+                uint32_t g = takeGrid(d, c);
                 d.grid[node] = g;
-                atomicAdd(&c->numGrids, 1u);
-                atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset),
-                          (unsigned long long)refAllocSize(kGridBytes));
                 d.splitIter[node] = stamp2;
                 if (g != kNone) {
                     const uint32_t zi = atomicAdd(&c->numZero, 1u);
@@ -953,10 +967,8 @@ __device__ __forceinline__ void makeChild(const Dev& d, uint32_t ch, uint32_t pa
 __device__ __forceinline__ void bookSplit(const Dev& d, Counters* c, uint32_t node, uint32_t stamp) {
     uint32_t g = d.grid[node];
     if (g == kNone) {
-        g = arenaAlloc(d, kGridUnits);
+        g = takeGrid(d, c);
         d.grid[node] = g;
-        atomicAdd(&c->numGrids, 1u);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset), (unsigned long long)refAllocSize(kGridBytes));
     }
     d.splitIter[node] = stamp;
     if (g != kNone) {
@@ -2396,6 +2408,205 @@ __global__ void k_deepen_end(Dev d) {
     if (c->numAllocatedChunks > c->chunkPoolSize) c->chunkPoolSize = c->numAllocatedChunks;
     c->spilledPointsTotal += c->numSpilled;
     if (c->iter > d.maxExpandIters) c->arrivalMode = 1u;
+    settleGridPool(c);
+}
+
+// Refinement's collapsing (wiki/02_KernelPipeline.md:228-243, "merge a node
+// back up", listed by the reference and not built there: it needs somewhere
+// to return the 256 KB grid, CLAUDE.md:185-187). A node whose eight children
+// are all leaves, holding at most maxPoints points between them, becomes a
+// leaf again with all their points: its chunks are allocated first (recycled
+// queue chunks, then fresh ones, charged as a batch's are), the children's
+// points are copied in, then the children's chunks return to the queue, the
+// children become empty unreachable leaves (the pool only grows, as the
+// reference's does), the node drops its voxels (their chunks are not reused)
+// and its grid goes to the grid pool, where the next split takes it. The
+// node's exact sums restart from zero and it is marked dirty, so Accumulate
+// folds all its points. Candidates come from the caller (d.spillNodes).
+constexpr uint32_t kCollapseMax = 4096;
+
+// Sorts the candidates, drops duplicates and ineligible nodes, books each
+// merged leaf's chunks. One block. Records in splitRecs: node, numPoints (its
+// points), chunkBase (its first copy item), numChunks (its children's chunks),
+// grid, queueBase (its first allocation index), spillBase (chunks it needs).
+__global__ void __launch_bounds__(1024) k_collapse_plan(Dev d, uint32_t count, uint32_t maxPoints) {
+    __shared__ uint32_t s_ids[kCollapseMax];
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_fresh;
+    Counters* c = d.ctr;
+    const uint32_t n = count < kCollapseMax ? count : kCollapseMax;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) s_ids[i] = d.spillNodes[i];
+    __syncthreads();
+    bitonicSort(s_ids, n);
+    const uint32_t nn = c->numNodes, ppc = d.ppc;
+    const uint32_t maxPts = maxPoints ? maxPoints : d.maxPointsPerNode;
+    uint32_t sel = 0, reqRun = 0, ownRun = 0;
+    for (uint32_t b = 0; b < n; b += blockDim.x) {
+        const uint32_t i = b + threadIdx.x;
+        const uint32_t node = i < n ? s_ids[i] : kNone;
+        uint32_t take = 0, total = 0, owned = 0;
+        if (node < nn && (i == 0 || s_ids[i - 1] != node) && d.level[node] > 0u && !isLeaf(d, node)) {
+            take = 1;
+            for (uint32_t q = 0; q < 8u; q++) {
+                const int32_t ch = d.child[node * 8u + q];
+                if (ch < 0 || (uint32_t)ch >= nn || !isLeaf(d, (uint32_t)ch)) {
+                    take = 0;
+                    break;
+                }
+                const uint32_t oc = d.numPointChunks[ch], np = d.numPoints[ch];
+                total += np < oc * ppc ? np : oc * ppc;
+                owned += oc;
+            }
+            if (total > maxPts) take = 0;
+        }
+        const uint32_t req = take ? (total + ppc - 1u) / ppc : 0u;
+        uint32_t tSel, tReq, tOwn;
+        const uint32_t pSel = blockExclusiveScan(take, &tSel, s_warp);
+        const uint32_t pReq = blockExclusiveScan(req, &tReq, s_warp);
+        const uint32_t pOwn = blockExclusiveScan(take ? owned : 0u, &tOwn, s_warp);
+        if (take) {
+            SplitRec r;
+            r.node = node;
+            r.numPoints = total;
+            r.tableOff = kNone;
+            r.spillBase = req;
+            r.chunkBase = ownRun + pOwn;
+            r.numChunks = owned;
+            r.grid = d.grid[node];
+            r.queueBase = reqRun + pReq;
+            d.splitRecs[sel + pSel] = r;
+            atomicAdd(&c->collapsePoints, (unsigned long long)total);
+        }
+        sel += tSel;
+        reqRun += tReq;
+        ownRun += tOwn;
+    }
+    // the merged leaves' chunks: logical queue positions [A, A + reqRun),
+    // recycled below the pool's size, fresh from the arena at and above it
+    const uint32_t A = c->numAllocatedChunks, pool = c->chunkPoolSize;
+    const uint32_t firstFresh = A > pool ? A : pool;
+    const uint32_t fresh = A + reqRun > firstFresh ? A + reqRun - firstFresh : 0u;
+    if (threadIdx.x == 0) {
+        s_fresh = kNone;
+        if (fresh) {
+            s_fresh = arenaAlloc(d, fresh * d.ptChunkUnits);
+            atomicAdd(&c->numPtChunks, fresh);
+            c->refOffset += (unsigned long long)fresh * refAllocSize(kRefChunkBytes);
+        }
+        c->collapseSelected = sel;
+        c->collapseItems = ownRun;
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < sel; k += blockDim.x) {
+        const SplitRec r = d.splitRecs[k];
+        const uint32_t req = r.spillBase;
+        if (req && ensureTable(d, d.ptTableOff, d.ptTableCap, r.node, req, 0u)) {
+            const uint32_t off = d.ptTableOff[r.node];
+            for (uint32_t e = 0; e < req; e++) {
+                const uint32_t idx = A + r.queueBase + e;
+                uint32_t phys;
+                if (idx < pool) phys = idx < d.maxPtChunks ? d.chunkQueue[idx] : kNone;
+                else phys = s_fresh == kNone ? kNone : s_fresh + (idx - firstFresh) * d.ptChunkUnits;
+                d.tablePool[off + e] = phys;
+            }
+            d.numPointChunks[r.node] = req;
+        }
+        d.numPoints[r.node] = r.numPoints;
+        d.counter[r.node] = r.numPoints;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c->numAllocatedChunks = A + reqRun;
+        if (c->numAllocatedChunks > c->chunkPoolSize) c->chunkPoolSize = c->numAllocatedChunks;
+    }
+}
+
+// The children's points into the merged leaves: one work item per child
+// chunk, the destination slot the child's offset among its siblings plus the
+// slot in the child. The children's tables are intact until k_collapse_finish.
+__global__ void __launch_bounds__(256) k_collapse_copy(Dev d) {
+    const Counters* c = d.ctr;
+    const uint32_t sel = c->collapseSelected, items = c->collapseItems, ppc = d.ppc;
+    for (uint32_t w = blockIdx.x; w < items; w += gridDim.x) {
+        uint32_t lo = 0, hi = sel;
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (d.splitRecs[mid].chunkBase <= w) lo = mid;
+            else hi = mid;
+        }
+        const SplitRec r = d.splitRecs[lo];
+        uint32_t j = w - r.chunkBase, base = 0, ch = kNone;
+        for (uint32_t q = 0; q < 8u; q++) {
+            const uint32_t cq = (uint32_t)d.child[r.node * 8u + q];
+            const uint32_t oc = d.numPointChunks[cq];
+            if (j < oc) {
+                ch = cq;
+                break;
+            }
+            j -= oc;
+            const uint32_t np = d.numPoints[cq];
+            base += np < oc * ppc ? np : oc * ppc;
+        }
+        if (ch == kNone) continue;
+        const uint32_t oc = d.numPointChunks[ch];
+        const uint32_t np = d.numPoints[ch] < oc * ppc ? d.numPoints[ch] : oc * ppc;
+        const uint32_t first = j * ppc, last = first + ppc < np ? first + ppc : np;
+        const uint32_t src = d.tablePool[d.ptTableOff[ch] + j];
+        const uint32_t dcap = d.numPointChunks[r.node] * ppc;
+        if (src == kNone) continue;
+        for (uint32_t s = first + threadIdx.x; s < last; s += blockDim.x) {
+            const uint32_t slot = base + s;
+            if (slot >= dcap) continue;
+            const uint32_t dst = d.tablePool[d.ptTableOff[r.node] + slot / ppc];
+            if (dst == kNone) continue;
+            chunkPoints(d, dst)[slot % ppc] = chunkPoints(d, src)[s - first];
+            chunkIndices(d, dst)[slot % ppc] = chunkIndices(d, src)[s - first];
+        }
+    }
+}
+
+// The children's chunks back to the queue (after the merged leaves took
+// theirs), the children emptied, the merged nodes' voxels dropped and their
+// grids into the pool; dirty marks for Accumulate. One block.
+__global__ void __launch_bounds__(1024) k_collapse_finish(Dev d) {
+    Counters* c = d.ctr;
+    const uint32_t sel = c->collapseSelected, own = c->collapseItems;
+    const uint32_t A = c->numAllocatedChunks, qbase = A - own;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < sel; k += blockDim.x) {
+        const SplitRec r = d.splitRecs[k];
+        uint32_t pos = qbase + r.chunkBase;
+        AccumI z = {};
+        for (uint32_t q = 0; q < 8u; q++) {
+            const uint32_t ch = (uint32_t)d.child[r.node * 8u + q];
+            const uint32_t oc = d.numPointChunks[ch];
+            for (uint32_t j = 0; j < oc; j++, pos++)
+                if (pos < d.maxPtChunks) d.chunkQueue[pos] = d.tablePool[d.ptTableOff[ch] + j];
+            d.numPoints[ch] = 0;
+            d.counter[ch] = 0;
+            d.numPointChunks[ch] = 0;
+            d.ptTableOff[ch] = kNone;
+            d.ptTableCap[ch] = 0;
+            d.accum[ch] = z;
+            d.child[r.node * 8u + q] = -1;
+        }
+        atomicAdd(&c->collapseVoxels, (unsigned long long)d.numVoxels[r.node]);
+        d.numVoxels[r.node] = 0;
+        d.numVoxelsStored[r.node] = 0;
+        d.numVoxelChunks[r.node] = 0;
+        d.vxTableOff[r.node] = kNone;
+        d.vxTableCap[r.node] = 0;
+        d.splitIter[r.node] = 0;
+        d.accum[r.node] = z;
+        if (r.grid != kNone) {
+            d.gridPool[atomicAdd(&c->gridPoolSize, 1u)] = r.grid;
+            d.grid[r.node] = kNone;
+            atomicSub(&c->numGrids, 1u);
+        }
+        markDirty(d, r.node);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) c->numAllocatedChunks = qbase;
 }
 
 // n == kNone: the batch at the device cursor.
@@ -2410,6 +2621,7 @@ __global__ void k_batch_end(Dev d, uint32_t n) {
     c->spilledPointsTotal += c->numSpilled;
     c->expandIters += c->iter < d.maxExpandIters ? c->iter : d.maxExpandIters;
     if (c->iter > d.maxExpandIters) c->arrivalMode = 1u;
+    settleGridPool(c);
 }
 
 // Stats sweep (remolod_octree.cu:1271-1310).
@@ -2484,6 +2696,11 @@ void launchDeepenBegin(const Dev& d, const uint32_t* queue, uint32_t queueLen, u
     k_deepen_begin<<<1, 1024, 0, s>>>(d, queue, queueLen, budget, minPoints);
 }
 void launchDeepenEnd(const Dev& d, cudaStream_t s) { k_deepen_end<<<1, 1, 0, s>>>(d); }
+void launchCollapse(const Dev& d, uint32_t count, uint32_t maxPoints, int grid, cudaStream_t s) {
+    k_collapse_plan<<<1, 1024, 0, s>>>(d, count, maxPoints);
+    k_collapse_copy<<<grid, 256, 0, s>>>(d);
+    k_collapse_finish<<<1, 1024, 0, s>>>(d);
+}
 void launchCountFirst(const Dev& d, const Point* pts, uint32_t n, int grid, cudaStream_t s) {
     k_count_first<<<grid, 256, 0, s>>>(d, pts, n);
 }

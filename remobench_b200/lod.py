@@ -266,6 +266,15 @@ class Context:
         self._ok(capi.lib().rb_refine_deepen(self.h, int(budget), int(min_points), ctypes.byref(r)))
         return r
 
+    def refine_collapse(self, nodes, max_points=0):
+        """Collapsing of the given nodes whose children are all leaves
+        (rb_refine_collapse): each becomes a leaf with its children's points."""
+        arr = np.ascontiguousarray(nodes, dtype=np.uint32)
+        r = capi.CollapseResult()
+        self._ok(capi.lib().rb_refine_collapse(self.h, ctypes.c_void_p(arr.ctypes.data) if len(arr) else None,
+                                               len(arr), int(max_points), ctypes.byref(r)))
+        return r
+
     def set_stream(self, stream_handle):
         self._ok(capi.lib().rb_set_stream(self.h, ctypes.c_void_p(int(stream_handle))))
 

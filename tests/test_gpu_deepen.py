@@ -119,3 +119,63 @@ def test_deepen_needs_analysis_and_respects_the_pool(c1_cloud):
         ctx.refine_deepen(8)
     ctx.close()
     tree.close()
+
+
+def test_collapse_undoes_deepening_and_matches_oracle(c1_cloud):
+    """Refinement's collapsing (wiki/02_KernelPipeline.md:228-243, "merge a
+    node back up") on the B200 against the oracle: the leaves a deepening pass
+    split are twigs (eight leaf children under the split limit), and
+    collapsing them merges their points back, drops their voxels and returns
+    their grids to the pool. Tree, points, voxels, grids, accumulators and the
+    pre-EDL framebuffer equal the oracle's; two more batches then split nodes
+    with the pooled grids, and the trees still agree."""
+    import torch
+    from test_gpu_analysis import oracle_frame
+    from remobench_b200.lod import Context, DeviceRing, make_frame
+    cfg, cloud, bmin, bmax = c1_cloud
+    bs = cfg.batch_size
+    ctx = Context(slot_capacity=bs, time_budget_ms=0.0)
+    ctx.allocate(len(cloud), bmin, bmax)
+    ring = DeviceRing(cloud, bs, slots=ctx.cfg.ring_slots, slot_capacity=bs)
+    ring.upload_window(0)
+    assert ctx.build(ring.ring, ring.sizes, 6, ring.num_batches).batches_consumed == 6
+    tree = ob.Tree()
+    tree.reset(bmin, bmax)
+    for b in range(6):
+        assert tree.add_batch(cloud[b * bs:(b + 1) * bs]) == 0
+    tree.accumulate(6)
+    f = make_frame(bmin, bmax, W, H, yaw=1.2, pitch=-0.5, radius_scale=0.5)
+    ctx.analyze(f, min_points=16, closure_margin=8, frontier_only=False, queue_capacity=4096)
+    queue = ctx.queue()
+    d = ctx.refine_deepen(64)
+    assert tree.deepen(queue[:64])[1] == d.nodes_selected > 0
+    tree.accumulate(6)
+    nodes = ctx.nodes()
+    twigs = [i for i in range(1, len(nodes)) if not nodes["is_leaf"][i]
+             and np.all(nodes["child"][i] >= 0) and np.all(nodes["is_leaf"][nodes["child"][i]] == 1)
+             and int(nodes["num_points"][nodes["child"][i]].sum()) <= 50000]
+    assert len(twigs) == d.nodes_selected
+    grids_before = ctx.stats().num_grids
+    r = ctx.refine_collapse(twigs + twigs[:3])
+    m, moved, dropped = tree.collapse(twigs + twigs[:3])
+    assert (r.nodes_collapsed, r.points_moved, r.voxels_dropped) == (m, moved, dropped)
+    assert r.nodes_collapsed == len(twigs) and r.grids_returned == len(twigs)
+    tree.accumulate(6)
+    tree.sweep()
+    compare_all(ctx, tree)
+    assert ctx.stats().num_grids == grids_before - len(twigs)
+    # the emptied children are reachable from no node and draw nothing
+    fb = torch.empty(W * H, dtype=torch.int64, device="cuda")
+    rr = ctx.render(f, fb)
+    ofb, orr, _ = tree.render(oracle_frame(f))
+    assert (rr.draw_items, rr.draw_samples) == (orr.draw_items, orr.draw_samples)
+    assert np.array_equal(fb.cpu().numpy().view(np.uint64), ofb)
+
+    assert ctx.build(ring.ring, ring.sizes, 8, ring.num_batches).batches_consumed == 8
+    for b in range(6, 8):
+        assert tree.add_batch(cloud[b * bs:(b + 1) * bs]) == 0
+    tree.accumulate(8)
+    tree.sweep()
+    compare_all(ctx, tree)
+    ctx.close()
+    tree.close()

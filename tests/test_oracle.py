@@ -316,3 +316,74 @@ def test_deepen_keeps_every_point_and_samples_the_deepened_nodes(c1_cloud):
     for i in pick:
         assert after["is_leaf"][i] == 0 and after["num_voxels"][i] > 0
         assert after["num_voxels"][i] == int(sum(bin(int(w)).count("1") for w in t.node_grid(int(i))))
+
+
+def twigs(nodes, limit=50000):
+    """Nodes below the root whose eight children are all leaves, holding at
+    most `limit` points together."""
+    out = []
+    for i in range(1, len(nodes)):
+        kids = nodes["child"][i]
+        if nodes["is_leaf"][i] or np.any(kids < 0):
+            continue
+        if np.all(nodes["is_leaf"][kids] == 1) and int(nodes["num_points"][kids].sum()) <= limit:
+            out.append(i)
+    return out
+
+
+def test_collapse_merges_twigs_and_later_splits_reuse_their_grids(c1_cloud):
+    cfg, cloud, bmin, bmax = c1_cloud
+    t = ob.Tree(num_threads=4)
+    t.reset(bmin, bmax)
+    bs = cfg.batch_size
+    for b in range(6):
+        assert t.add_batch(cloud[b * bs:(b + 1) * bs]) == 0
+    t.sweep()
+    # a normally built tree has no twig under the split limit (a node splits
+    # only past it); deepened leaves are twigs: collapsing undoes deepening
+    nodes = t.node_table()
+    leaves = np.nonzero(nodes["is_leaf"] & (nodes["num_points"] > 0))[0]
+    pick = [int(i) for i in leaves[np.argsort(-nodes["num_points"][leaves], kind="stable")][:10]]
+    assert not twigs(nodes)
+    held = {i: np.sort(t.leaf_points(i)[1]) for i in pick}
+    assert t.deepen(pick) == (False, len(pick))
+    t.sweep()
+    nodes = t.node_table()
+    cand = twigs(nodes)
+    assert sorted(cand) == sorted(pick)
+    before = t.stats()
+    kids = {i: list(nodes["child"][i]) for i in cand}
+    want = {i: int(nodes["num_points"][kids[i]].sum()) for i in cand}
+    m, moved, dropped = t.collapse(cand + cand[:2])  # duplicates are ignored
+    assert m == len(cand) and moved == sum(want.values())
+    assert dropped == int(nodes["num_voxels"][cand].sum())
+    t.sweep()
+    s = t.stats()
+    assert s.num_grids == before.num_grids - len(cand)
+    after = t.node_table()
+    for i in cand:
+        assert after["is_leaf"][i] == 1 and after["num_points"][i] == want[i] and after["num_voxels"][i] == 0
+        assert after["grid"][i] < 0
+        assert np.array_equal(np.sort(t.leaf_points(i)[1]), held[i])
+        assert np.all(after["num_points"][kids[i]] == 0)
+    # every point still stored once, with its global index
+    seen = np.zeros(6 * bs, dtype=np.int32)
+    for i in np.nonzero(after["is_leaf"])[0]:
+        seen[t.leaf_points(int(i))[1]] += 1
+    assert np.all(seen == 1)
+    g = t.accumulate(6)
+    assert g.sum_leaf_counts == 6 * bs and g.inner_with_sums == 0
+    # later batches split again and take the returned grids first
+    grids_before = len(np.unique(after["grid"][after["grid"] >= 0]))
+    for b in range(6, 8):
+        assert t.add_batch(cloud[b * bs:(b + 1) * bs]) == 0
+    t.sweep()
+    s2 = t.stats()
+    assert s2.num_points == len(cloud) and s2.dropped_points == 0
+    fin = t.node_table()
+    used = np.unique(fin["grid"][fin["grid"] >= 0])
+    assert len(used) == s2.num_grids and len(used) >= grids_before
+    seen = np.zeros(len(cloud), dtype=np.int32)
+    for i in np.nonzero(fin["is_leaf"])[0]:
+        seen[t.leaf_points(int(i))[1]] += 1
+    assert np.all(seen == 1)

@@ -2767,8 +2767,8 @@ void launchResetRoot(const Dev& d, int grid, cudaStream_t s) { k_reset_root<<<gr
 // One batch as a CUDA graph: the phase kernels of runBatch, every kernel
 // reading its batch from the device cursor, the expand round's leftovers in
 // the cooperative k_expand_rest. After it the graph forks: the voxel path
-// (k_vox_sample or, after a lost cell, k_vox_sample_levels; k_vox_lift,
-// k_vox_commit, k_alloc_voxels, k_vox_store) and the point path
+// (k_vox_sample, or after a lost cell k_vox_sample_levels on a branch of its
+// own; k_vox_lift, k_vox_commit, k_alloc_voxels, k_vox_store) and the point path
 // (k_alloc_points, k_insert) read the finished tree and write disjoint node
 // fields and chunks, so the point path runs in the voxel path's shadow; they
 // join before k_batch_end. One graph launch builds the batch at batchletIndex
@@ -2776,13 +2776,15 @@ void launchResetRoot(const Dev& d, int grid, cudaStream_t s) { k_reset_root<<<gr
 // no batch uploaded, time budget) runs through as no-ops.
 cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int restGrid, cudaGraphExec_t* out) {
     *out = nullptr;
-    cudaStream_t cs = nullptr, cs2 = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t cs = nullptr, cs2 = nullptr, cs3 = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr, joinLevels = nullptr;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs3, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&joinLevels, cudaEventDisableTiming);
     bool capturing = false;
     while (e == cudaSuccess) {
         if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) break;
@@ -2799,8 +2801,13 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int re
         k_alloc_points<<<fixedGrid, 256, 0, cs2>>>(d);
         k_insert<<<pointGrid, 256, 0, cs2>>>(d, nullptr, 0u);
         if ((e = cudaEventRecord(join, cs2)) != cudaSuccess) break;
+        // the two forms of voxel sampling exclude each other (Counters::levelMode):
+        // the one that returns at once runs beside the other, off the path
+        if ((e = cudaStreamWaitEvent(cs3, fork, 0)) != cudaSuccess) break;
+        k_vox_sample_levels<<<pointGrid, 256, 0, cs3>>>(d, nullptr, 0u);
+        if ((e = cudaEventRecord(joinLevels, cs3)) != cudaSuccess) break;
         k_vox_sample<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
-        k_vox_sample_levels<<<pointGrid, 256, 0, cs>>>(d, nullptr, 0u);
+        if ((e = cudaStreamWaitEvent(cs, joinLevels, 0)) != cudaSuccess) break;
         k_vox_lift<<<pointGrid, kLiftThreads, 0, cs>>>(d);
         k_vox_commit<<<fixedGrid, 256, 0, cs>>>(d);
         k_alloc_voxels<<<fixedGrid, 256, 0, cs>>>(d);
@@ -2820,8 +2827,10 @@ cudaError_t captureBatchGraph(const Dev& d, int pointGrid, int fixedGrid, int re
     }
     if (graph) cudaGraphDestroy(graph);
     if (join) cudaEventDestroy(join);
+    if (joinLevels) cudaEventDestroy(joinLevels);
     if (fork) cudaEventDestroy(fork);
     if (cs2) cudaStreamDestroy(cs2);
+    if (cs3) cudaStreamDestroy(cs3);
     if (cs) cudaStreamDestroy(cs);
     if (e != cudaSuccess) {
         cudaGetLastError();

@@ -1109,6 +1109,25 @@ __global__ void __launch_bounds__(1024) k_deep_book(Dev d) {
     if (threadIdx.x == 0) deepBookCounters(d, c, ns, acc, spilledBefore, totPts, totCh, stamp, levels, n0);
 }
 
+// The depths of the expand round's pyramid that are counted point by point:
+// the odd ones and the deepest. Every other depth is one below a counted one,
+// so its count is the sum of eight counted cubes (deepCount): three rounds of
+// binning per point instead of five.
+__device__ __forceinline__ bool deepBinned(uint32_t depth, uint32_t levels) {
+    return (depth & 1u) != 0u || depth == levels;
+}
+
+// The points in cube `code` at `depth` below root slot `slot`.
+__device__ __forceinline__ uint32_t deepCount(const Dev& d, uint32_t slot, uint32_t depth, uint32_t code,
+                                              uint32_t levels) {
+    const uint32_t* row = d.deepCnt + (size_t)slot * kDeepCells;
+    if (deepBinned(depth, levels)) return row[deepOffset(depth) + code];
+    // the eight cubes one depth down are contiguous (code << 3 | octant)
+    const uint4* k = reinterpret_cast<const uint4*>(row + deepOffset(depth + 1u) + (code << 3));
+    const uint4 a = k[0], b = k[1];
+    return a.x + a.y + a.z + a.w + b.x + b.y + b.z + b.w;
+}
+
 // A block's bin counts, merged in shared memory before they reach the global
 // bins: the coarse cubes (8 per root at depth 1) are shared by most of a
 // batch's points, and one global atomic per warp on them serialises in one L2
@@ -1135,7 +1154,9 @@ __device__ __forceinline__ void deepBinsFlush(const Dev& d, DeepBlockBins& b) {
 // One point below root slot `slot` (at level lv) into its cubes at depths
 // 1..levels. Every lane of the warp calls it; lanes with no point pass
 // active = false. Equal cubes in a warp add once, into the block's table
-// (or straight into the global bin when its probe run is full).
+// (or straight into the global bin when its probe run is full). Only the
+// depths deepBinned names are counted; a cube at another depth holds the
+// points of its eight cubes one depth down (deepCount).
 __device__ __forceinline__ void deepBin(const Dev& d, DeepBlockBins& bins, bool active, uint32_t slot, uint32_t lv,
                                         const Point& p, uint32_t levels) {
     uint32_t x = 0, y = 0, z = 0;
@@ -1149,6 +1170,7 @@ __device__ __forceinline__ void deepBin(const Dev& d, DeepBlockBins& bins, bool 
     for (uint32_t j = 1; j <= kDeepLevels; j++) {
         if (j > levels) break;  // the same for every lane
         code = (code << 3) | (active ? childIndex(x, y, z, lv + j - 1u) : 0u);
+        if (!deepBinned(j, levels)) continue;  // the same for every lane
         const uint32_t key = active ? slot * kDeepCells + deepOffset(j) + code : kNone;
         const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
         if (active && (int)laneId() == __ffs(peers) - 1) {
@@ -1273,7 +1295,7 @@ __global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
             uint32_t cnt = 0;
             if (node < hi) {
                 const uint32_t meta = d.deepMeta[node - base];
-                cnt = d.deepCnt[(meta >> 16) * kDeepCells + deepOffset(g) + (meta & 0xFFFFu)];
+                cnt = deepCount(d, meta >> 16, g, meta & 0xFFFFu, levels);
                 d.counter[node] = cnt;
             }
             const bool over = node < hi && cnt > d.maxPointsPerNode;

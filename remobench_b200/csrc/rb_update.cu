@@ -509,9 +509,12 @@ __device__ __forceinline__ uint32_t warpSortAscending(uint32_t v) {
 // reference's allocator charges it. Pool grids are zeroed with the others.
 __device__ __forceinline__ uint32_t takeGrid(const Dev& d, Counters* c) {
     atomicAdd(&c->numGrids, 1u);
-    const uint32_t k = atomicAdd(&c->gridPoolTaken, 1u);
+    // the pool's size changes only between batches
     const uint32_t pool = c->gridPoolSize;
-    if (k < pool) return d.gridPool[pool - 1u - k];
+    if (pool != 0u) {
+        const uint32_t k = atomicAdd(&c->gridPoolTaken, 1u);
+        if (k < pool) return d.gridPool[pool - 1u - k];
+    }
     atomicAdd(reinterpret_cast<unsigned long long*>(&c->refOffset), (unsigned long long)refAllocSize(kGridBytes));
     return arenaAlloc(d, kGridUnits);
 }
@@ -926,7 +929,14 @@ __global__ void __launch_bounds__(256) k_spill_copy(Dev d, uint32_t gated) { spi
 // A new node: child `i` of `parent` at id `ch` (doSplitting's child set-up,
 // remolod_octree.cu:323-347), with its ancestor row.
 __device__ __forceinline__ void makeChild(const Dev& d, uint32_t ch, uint32_t parent, uint32_t i) {
+    // the parent's fields and its whole ancestor row in one round of loads
+    // (row entries at and past its level are read and ignored)
     const uint32_t plv = d.level[parent], pg = d.grid[parent];
+    const uint32_t px = d.nodeX[parent], py = d.nodeY[parent], pz = d.nodeZ[parent];
+    const uint2* prow = d.anc + (size_t)parent * kMaxDepth;
+    uint2 arow[kMaxDepth];
+#pragma unroll
+    for (uint32_t l = 0; l < (uint32_t)kMaxDepth; l++) arow[l] = prow[l];
     const uint32_t lv = plv + 1u;
 #pragma unroll
     for (int q = 0; q < 8; q++) d.child[ch * 8u + q] = -1;
@@ -935,9 +945,9 @@ __device__ __forceinline__ void makeChild(const Dev& d, uint32_t ch, uint32_t pa
     reinterpret_cast<uint4*>(d.hist8 + (size_t)ch * 8u)[1] = make_uint4(0, 0, 0, 0);
     d.numPoints[ch] = 0;
     d.level[ch] = lv;
-    d.nodeX[ch] = 2u * d.nodeX[parent] + ((i >> 2) & 1u);
-    d.nodeY[ch] = 2u * d.nodeY[parent] + ((i >> 1) & 1u);
-    d.nodeZ[ch] = 2u * d.nodeZ[parent] + (i & 1u);
+    d.nodeX[ch] = 2u * px + ((i >> 2) & 1u);
+    d.nodeY[ch] = 2u * py + ((i >> 1) & 1u);
+    d.nodeZ[ch] = 2u * pz + (i & 1u);
     d.grid[ch] = kNone;
     d.numVoxels[ch] = 0;
     d.numVoxelsStored[ch] = 0;
@@ -951,11 +961,10 @@ __device__ __forceinline__ void makeChild(const Dev& d, uint32_t ch, uint32_t pa
     d.dirtyStamp[ch] = 0;
     AccumI z = {};
     d.accum[ch] = z;
-    const uint2* prow = d.anc + (size_t)parent * kMaxDepth;
     uint2* crow = d.anc + (size_t)ch * kMaxDepth;
 #pragma unroll
     for (uint32_t l = 0; l < (uint32_t)kMaxDepth; l++)
-        if (l + 1u < lv) crow[l] = prow[l];
+        if (l + 1u < lv) crow[l] = arow[l];
     crow[lv - 1u] = make_uint2(parent, pg);
     d.parent[ch] = make_uint2(parent, pg);
     d.child[parent * 8u + i] = (int32_t)ch;
@@ -964,39 +973,47 @@ __device__ __forceinline__ void makeChild(const Dev& d, uint32_t ch, uint32_t pa
 // The bookkeeping every split shares: a grid if the node has none (allocated
 // once, zeroed at every split, :365-387), its split stamp, the grid on the
 // zero list and the node on the dirty list.
-__device__ __forceinline__ void bookSplit(const Dev& d, Counters* c, uint32_t node, uint32_t stamp) {
+__device__ __forceinline__ uint32_t bookSplit(const Dev& d, Counters* c, uint32_t node, uint32_t stamp) {
+    // The node's fields in one round of loads, then the counter atomics back
+    // to back: the single-block kernels that call this are bound by their
+    // chain of dependent round trips. Every split takes a zero-list slot; one
+    // left without a grid (arena exhausted) holds kNone and is skipped.
     uint32_t g = d.grid[node];
+    const uint32_t bs = c->buildStamp;
+    const bool dirty = d.dirtyStamp[node] == bs;
+    const uint32_t z = atomicAdd(&c->numZero, 1u);
+    const uint32_t di = dirty ? kNone : atomicAdd(&c->numDirty, 1u);
     if (g == kNone) {
         g = takeGrid(d, c);
         d.grid[node] = g;
     }
     d.splitIter[node] = stamp;
-    if (g != kNone) {
-        const uint32_t z = atomicAdd(&c->numZero, 1u);
-        if (z < d.zeroCap) d.zeroList[z] = g;
-    }
-    if (d.dirtyStamp[node] != c->buildStamp) {
-        d.dirtyStamp[node] = c->buildStamp;
-        const uint32_t di = atomicAdd(&c->numDirty, 1u);
+    if (z < d.zeroCap) d.zeroList[z] = g;
+    if (!dirty) {
+        d.dirtyStamp[node] = bs;
         if (di < d.maxNodes) d.dirtyList[di] = node;
     }
+    return g;
 }
 
 // Root k of the round: its split bookkeeping and its record for k_deep_bin
 // (spill slots from prePts, copy items from preCh).
 __device__ __forceinline__ void deepBookRoot(const Dev& d, Counters* c, uint32_t k, uint32_t node, uint32_t np,
                                              uint32_t owned, uint32_t spillBase, uint32_t chunkBase, uint32_t stamp) {
-    bookSplit(d, c, node, stamp);
+    // issued ahead of the split's own atomics, used after them
+    const uint32_t tableOff = d.ptTableOff[node];
+    // the node's chunks go back to the queue (remolod_octree.cu:349-360)
+    const uint32_t queueBase = owned ? atomicSub(&c->numAllocatedChunks, owned) - owned : kNone;
+    const uint32_t g = bookSplit(d, c, node, stamp);
     SplitRec r;
     r.node = node;
     r.numPoints = np;
-    r.tableOff = d.ptTableOff[node];
+    r.tableOff = tableOff;
     r.spillBase = spillBase;
     r.chunkBase = chunkBase;
     r.numChunks = owned;
-    r.grid = d.grid[node];
-    // the node's chunks go back to the queue (remolod_octree.cu:349-360)
-    r.queueBase = owned ? atomicSub(&c->numAllocatedChunks, owned) - owned : kNone;
+    r.grid = g;
+    r.queueBase = queueBase;
     d.splitRecs[k] = r;
     d.numPoints[node] = 0;
     d.numPointChunks[node] = 0;
@@ -1058,16 +1075,19 @@ __global__ void __launch_bounds__(1024) k_deep_book(Dev d) {
         if (threadIdx.x >= 32u) return;
         const uint32_t lane = threadIdx.x;
         const uint32_t node = warpSortAscending(lane < ns ? d.spillNodes[lane] : kNone);
-        const uint32_t maxLevel = __reduce_max_sync(0xFFFFFFFFu, lane < acc ? d.level[node] : 0u);
+        // the root's level, chunks and points in one round of loads
+        uint32_t lvl = 0, np = 0, owned = 0;
+        if (lane < acc) {
+            lvl = d.level[node];
+            owned = d.numPointChunks[node];
+            const uint32_t stored = d.numPoints[node];
+            const uint32_t cap = owned * d.ppc;
+            np = stored < cap ? stored : cap;
+        }
+        const uint32_t maxLevel = __reduce_max_sync(0xFFFFFFFFu, lvl);
         if (maxLevel >= (uint32_t)kMaxDepth) return;
         const uint32_t depthRoom = (uint32_t)kMaxDepth - maxLevel;
         const uint32_t levels = depthRoom < kDeepLevels ? depthRoom : kDeepLevels;
-        uint32_t np = 0, owned = 0;
-        if (lane < acc) {
-            owned = d.numPointChunks[node];
-            const uint32_t cap = owned * d.ppc;
-            np = d.numPoints[node] < cap ? d.numPoints[node] : cap;
-        }
         uint32_t xp = np, xc = owned;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1392,7 +1412,9 @@ __device__ void zeroGridsBody(const Dev& d) {
     const uint4 z = make_uint4(0, 0, 0, 0);
     for (uint32_t w = blockIdx.x; w < nz * kPieces + deepItems; w += gridDim.x) {
         if (w < nz * kPieces) {
-            uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, d.zeroList[w / kPieces])) + (w % kPieces) * kPiece;
+            const uint32_t zg = d.zeroList[w / kPieces];
+            if (zg == kNone) continue;
+            uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, zg)) + (w % kPieces) * kPiece;
             for (uint32_t q = threadIdx.x; q < kPiece; q += blockDim.x) g[q] = z;
         } else {
             const uint32_t u0 = (w - nz * kPieces) * kPiece;

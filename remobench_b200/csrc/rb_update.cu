@@ -1381,8 +1381,9 @@ __global__ void __launch_bounds__(256) k_deep_move(Dev d, const Point* __restric
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const bool batchPt = i < n;
         uint32_t cur = batchPt ? d.leafOf[i] : d.spillLeaf[i - n];
-        if (d.splitIter[cur] != stamp) continue;
+        // issued beside the leaf id: most points of a batch sit in the roots
         const Point p = batchPt ? loadPoint(pts + i) : d.spillPts[i - n];
+        if (d.splitIter[cur] != stamp) continue;
         const uint32_t x = quant20(p.x, d.boxMin[0], d.octreeSize), y = quant20(p.y, d.boxMin[1], d.octreeSize),
                        z = quant20(p.z, d.boxMin[2], d.octreeSize);
         uint32_t lv = d.level[cur];

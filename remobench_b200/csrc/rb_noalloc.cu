@@ -5,9 +5,9 @@
 // place where it must not allocate -- a frame callback with a hard real-time
 // budget that cannot take the allocator's lock or risk an allocation failure
 // mid-frame, or an embedder that hands all device memory to its own pool after
-// start-up, so that a later cudaMalloc would fail. rb_render keeps its scratch
-// in the context and, when EDL is on, allocates a full-frame copy on first use;
-// this entry point does neither.
+// start-up, so that a later cudaMalloc would fail. rb_render renders through
+// per-context scratch that rb_allocate allocates with the tree; this entry
+// point needs none of it.
 //
 // Its scratch -- per-node visible/large flags, the draw list and the three
 // counters -- is one file-scope __device__ array of kScratchBytes (about 1 MB).

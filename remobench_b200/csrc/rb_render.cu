@@ -386,16 +386,18 @@ __device__ __forceinline__ float fbDepth(unsigned long long px) {
     return __uint_as_float((uint32_t)(px >> 32));
 }
 
-// remoApplyEDL (remo_framebuffer.cuh:78-122), reading a copy of the buffer so
-// the result does not depend on which neighbours were already shaded; libm
-// log2f/expf in place of the reference's __log2f/__expf.
+// remoApplyEDL (remo_framebuffer.cuh:78-122); libm log2f/expf in place of
+// the reference's __log2f/__expf. It may run in place (src == dst): a pixel
+// reads its neighbours' depths only, and shading rewrites a pixel's colour
+// half only, so the result does not depend on which neighbours were already
+// shaded.
 __global__ void __launch_bounds__(256) k_edl(const unsigned long long* src, unsigned long long* dst,
                                              uint32_t width, uint32_t height, float strength) {
     const uint64_t npx = (uint64_t)width * height;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < npx;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const unsigned long long pixel = src[i];
-        dst[i] = pixel;
+        if (dst != src) dst[i] = pixel;
         const int32_t x = (int32_t)(i % width), y = (int32_t)(i / width);
         const float depth = fbDepth(pixel);
         if (!(depth < 3.0e38f)) continue;

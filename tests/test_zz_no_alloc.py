@@ -73,8 +73,7 @@ def test_noalloc_render_matches_rb_render_twice_in_a_row(small_tree, edl):
 def test_noalloc_render_takes_no_device_memory(small_tree):
     """The claim itself: after one warm-up call (which only settles the
     caching of torch's own tensors below), EDL-on renders leave the device's
-    free memory unchanged. rb_render would allocate its full-frame EDL copy the
-    first time it shades a frame this large; this entry point does not."""
+    free memory unchanged: no call allocates, whatever the frame size."""
     import torch
     from remobench_b200.lod import make_frame
     ctx, bmin, bmax = small_tree

@@ -1438,12 +1438,13 @@ rb_status rb_refine_deepen(rb_ctx* c, uint32_t budget, uint32_t min_points, rb_d
     if (!c->allocated || c->cfg.pipeline == RB_PIPELINE_FLAT) return fail(c, RB_ERR_STATE, "no tree");
     if (!c->analyzed) return fail(c, RB_ERR_STATE, "refine before rb_analyze");
     if (out) std::memset(out, 0, sizeof(*out));
+    const uint32_t qlen = c->hostActr->queueLength;
+    if (budget == 0 || qlen == 0) return RB_OK;  // nothing to take: no pass
     RB_CUDA(c, cudaSetDevice(c->device));
     rb_status st = readCounters(c);
     if (st != RB_OK) return st;
     const uint64_t splitBefore = c->hostCtr->nodesSplit;
     const uint32_t nodesBefore = c->hostCtr->numNodes;
-    const uint32_t qlen = c->hostActr->queueLength;
     LAUNCH(c, K_DEEPEN, 1, rb::launchDeepenBegin(c->d, c->aqueue, qlen, budget, min_points, c->stream));
     bool stopped = false;
     // no batch points: every phase reads the spill list only

@@ -57,4 +57,4 @@ def loss_and_grad(params, x, t):
         y[:, 1], t[:, 1], reduction="none")
     loss = per.mean()
     loss.backward()
-    return float(loss), p.grad.numpy()
+    return float(loss.detach()), p.grad.numpy()

@@ -602,6 +602,9 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     ALLOC(d.hist8, (uint64_t)N * 8, "child-octant counts");
     ALLOC(d.arrive, N, "points reaching each leaf");
     ALLOC(d.deepCnt, (uint64_t)rb::kDeepRoots * rb::kDeepCells, "expand round bins");
+    ALLOC(d.deepNode, (uint64_t)rb::kDeepRoots * rb::kDeepCells, "expand round node table");
+    ALLOC(d.moveCode, cfg.slot_capacity, "expand round point codes");
+    ALLOC(d.spillCode, d.spillCap, "expand round spilled point codes");
     ALLOC(d.deepSlot, N, "expand round root slots");
     ALLOC(d.deepMeta, N, "expand round node codes");
     ALLOC(d.deepPar, N / 8u + 1u, "expand round split lists");
@@ -645,6 +648,7 @@ rb_status rb_allocate(rb_ctx* c, const rb_cloud_meta* meta, uint64_t budget) {
     RB_CUDA(c, cudaMemsetAsync(d.hashSlots, 0xFF, (size_t)hashSize * 16, c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.ctr, 0, sizeof(Counters), c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.deepCnt, 0, (size_t)rb::kDeepRoots * rb::kDeepCells * 4, c->stream));
+    RB_CUDA(c, cudaMemsetAsync(d.deepNode, 0xFF, (size_t)rb::kDeepRoots * rb::kDeepCells * 4, c->stream));
     RB_CUDA(c, cudaMemsetAsync(d.arrive, 0, (size_t)N * 4, c->stream));
     RB_CUDA(c, cudaMemsetAsync(c->refine.refSlot, 0xFF, (size_t)N * 4, c->stream));
     RB_CUDA(c, cudaMemsetAsync(c->refine.hashKeys, 0xFF, ((size_t)c->refine.hashMask + 1) * 8, c->stream));

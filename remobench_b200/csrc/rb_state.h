@@ -258,6 +258,9 @@ struct Dev {
     // slot; per node made by the round, (slot << 16) | its code below the root;
     // per generation, the nodes split in id order
     uint32_t* deepCnt;
+    uint32_t* deepNode;      // [kDeepRoots * kDeepCells] the node the round made for each cube, kNone elsewhere
+    uint32_t* moveCode;      // [slot capacity] each binned batch point's cube code at the round's deepest depth
+    uint32_t* spillCode;     // [spillCap] the same for the roots' stored points, by spill slot
     uint32_t* deepSlot;      // [maxNodes]
     uint32_t* deepMeta;      // [maxNodes]
     uint32_t* deepPar;       // [maxNodes / 8 + 1]

@@ -1178,7 +1178,7 @@ __device__ __forceinline__ void deepBinsFlush(const Dev& d, DeepBlockBins& b) {
 // depths deepBinned names are counted; a cube at another depth holds the
 // points of its eight cubes one depth down (deepCount).
 __device__ __forceinline__ void deepBin(const Dev& d, DeepBlockBins& bins, bool active, uint32_t slot, uint32_t lv,
-                                        const Point& p, uint32_t levels) {
+                                        const Point& p, uint32_t levels, uint32_t* codeOut) {
     uint32_t x = 0, y = 0, z = 0;
     if (active) {
         x = quant20(p.x, d.boxMin[0], d.octreeSize);
@@ -1209,6 +1209,8 @@ __device__ __forceinline__ void deepBin(const Dev& d, DeepBlockBins& bins, bool 
             if (!done) atomicAdd(&d.deepCnt[key], g);
         }
     }
+    // the cube at the deepest depth, for k_deep_move
+    if (active) *codeOut = code;
 }
 
 // The roots' stored points move to the spill list (remolod_octree.cu:250-285)
@@ -1251,7 +1253,7 @@ __global__ void __launch_bounds__(256) k_deep_bin(Dev d, const Point* __restrict
                 d.spillIdx[slot] = chunkIndices(d, phys)[s - first];
                 d.spillLeaf[slot] = r.node;
             }
-            deepBin(d, s_bins, active, lo, lv, q, levels);
+            deepBin(d, s_bins, active, lo, lv, q, levels, d.spillCode + (active ? slot : 0u));
         }
     }
     const uint32_t per = (((n + gridDim.x - 1u) / gridDim.x) + 31u) & ~31u;
@@ -1273,7 +1275,7 @@ __global__ void __launch_bounds__(256) k_deep_bin(Dev d, const Point* __restrict
             slot = d.deepSlot[leaf];
             lv = d.level[leaf];
         }
-        deepBin(d, s_bins, active, slot, lv, p, levels);
+        deepBin(d, s_bins, active, slot, lv, p, levels, d.moveCode + i);
     }
     __syncthreads();
     deepBinsFlush(d, s_bins);
@@ -1297,6 +1299,7 @@ __global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
     for (uint32_t t = threadIdx.x; t < 8u * roots; t += blockDim.x) {
         makeChild(d, base + t, d.splitRecs[t >> 3].node, t & 7u);
         d.deepMeta[t] = ((t >> 3) << 16) | (t & 7u);
+        d.deepNode[(size_t)(t >> 3) * kDeepCells + deepOffset(1u) + (t & 7u)] = base + t;
     }
     __syncthreads();
     uint32_t lo = base, hi = base + 8u * roots;
@@ -1351,7 +1354,9 @@ __global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
             const uint32_t parent = d.deepPar[t >> 3];
             const uint32_t pm = d.deepMeta[parent - base];
             makeChild(d, hi + t, parent, t & 7u);
-            d.deepMeta[hi + t - base] = (pm & 0xFFFF0000u) | (((pm & 0xFFFFu) << 3) | (t & 7u));
+            const uint32_t meta = (pm & 0xFFFF0000u) | (((pm & 0xFFFFu) << 3) | (t & 7u));
+            d.deepMeta[hi + t - base] = meta;
+            d.deepNode[(size_t)(meta >> 16) * kDeepCells + deepOffset(g + 1u) + (meta & 0xFFFFu)] = hi + t;
         }
         __syncthreads();
         lo = hi;
@@ -1370,28 +1375,33 @@ __global__ void __launch_bounds__(1024) k_deep_split(Dev d) {
 }
 
 // Every point the round moved -- batch points and spilled points whose leaf
-// is a root -- down the finished subtree to its leaf.
+// is a root -- to its leaf in the finished subtree: the deepest node the round
+// made along the point's cube path (k_deep_bin's code), read from the round's
+// node table at every depth at once instead of walking down from the root.
 __global__ void __launch_bounds__(256) k_deep_move(Dev d, const Point* __restrict__ pts, uint32_t n) {
     const Counters* c = d.ctr;
     if (c->batchStop || !c->deepActive) return;
     RB_BATCH_AT_CURSOR(d, pts, n);
-    const uint32_t stamp = c->deepStamp;
+    const uint32_t stamp = c->deepStamp, levels = c->deepLevels;
     const uint32_t ns = c->numSpilled < d.spillCap ? c->numSpilled : d.spillCap;
     const uint32_t total = n + ns;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const bool batchPt = i < n;
         uint32_t cur = batchPt ? d.leafOf[i] : d.spillLeaf[i - n];
         // issued beside the leaf id: most points of a batch sit in the roots
-        const Point p = batchPt ? loadPoint(pts + i) : d.spillPts[i - n];
+        const uint32_t code = batchPt ? d.moveCode[i] : d.spillCode[i - n];
         if (d.splitIter[cur] != stamp) continue;
-        const uint32_t x = quant20(p.x, d.boxMin[0], d.octreeSize), y = quant20(p.y, d.boxMin[1], d.octreeSize),
-                       z = quant20(p.z, d.boxMin[2], d.octreeSize);
-        uint32_t lv = d.level[cur];
-        while (lv < (uint32_t)kMaxDepth) {
-            const int32_t nx = d.child[cur * 8u + childIndex(x, y, z, lv)];
-            if (nx < 0) break;
-            cur = (uint32_t)nx;
-            lv += 1u;
+        const uint32_t* row = d.deepNode + (size_t)d.deepSlot[cur] * kDeepCells;
+        uint32_t ids[kDeepLevels];
+#pragma unroll
+        for (uint32_t j = 1; j <= kDeepLevels; j++)
+            ids[j - 1u] = j <= levels ? row[deepOffset(j) + (code >> (3u * (levels - j)))] : kNone;
+#pragma unroll
+        for (uint32_t j = kDeepLevels; j >= 1u; j--) {
+            if (ids[j - 1u] != kNone) {
+                cur = ids[j - 1u];
+                break;
+            }
         }
         if (batchPt) d.leafOf[i] = cur;
         else d.spillLeaf[i - n] = cur;
@@ -1410,17 +1420,20 @@ __device__ void zeroGridsBody(const Dev& d) {
     constexpr uint32_t kPieces = kGridWords / 4u / kPiece;
     const uint32_t deepUnits = (c->deepRoots * kDeepCells + 3u) / 4u;  // rows are contiguous from slot 0
     const uint32_t deepItems = (deepUnits + kPiece - 1u) / kPiece;
-    const uint4 z = make_uint4(0, 0, 0, 0);
-    for (uint32_t w = blockIdx.x; w < nz * kPieces + deepItems; w += gridDim.x) {
+    const uint4 z = make_uint4(0, 0, 0, 0), none = make_uint4(kNone, kNone, kNone, kNone);
+    for (uint32_t w = blockIdx.x; w < nz * kPieces + 2u * deepItems; w += gridDim.x) {
         if (w < nz * kPieces) {
             const uint32_t zg = d.zeroList[w / kPieces];
             if (zg == kNone) continue;
             uint4* g = reinterpret_cast<uint4*>(gridWordsAt(d, zg)) + (w % kPieces) * kPiece;
             for (uint32_t q = threadIdx.x; q < kPiece; q += blockDim.x) g[q] = z;
         } else {
-            const uint32_t u0 = (w - nz * kPieces) * kPiece;
-            uint4* g = reinterpret_cast<uint4*>(d.deepCnt);
-            for (uint32_t q = u0 + threadIdx.x; q < u0 + kPiece && q < deepUnits; q += blockDim.x) g[q] = z;
+            // the round's bins back to zero, its node table back to kNone
+            const uint32_t k = w - nz * kPieces;
+            const bool nodes = k >= deepItems;
+            const uint32_t u0 = (nodes ? k - deepItems : k) * kPiece;
+            uint4* g = reinterpret_cast<uint4*>(nodes ? d.deepNode : d.deepCnt);
+            for (uint32_t q = u0 + threadIdx.x; q < u0 + kPiece && q < deepUnits; q += blockDim.x) g[q] = nodes ? none : z;
         }
     }
 }

@@ -387,3 +387,49 @@ def test_collapse_merges_twigs_and_later_splits_reuse_their_grids(c1_cloud):
     for i in np.nonzero(fin["is_leaf"])[0]:
         seen[t.leaf_points(int(i))[1]] += 1
     assert np.all(seen == 1)
+
+
+def test_collapse_known_answer_and_the_grid_pool():
+    # The deepened child 1 of test_deepen_known_answer collapses back: a leaf
+    # again with its three points, no voxels, its grid in the pool. Four more
+    # points in its octant push it over the limit (4) and it splits again,
+    # taking the pooled grid: no new grid, no new store charge for one.
+    t = unit_tree(max_points_per_node=4)
+    cloud = pts([(0.1, 0.1, 0.1, 11), (0.3, 0.1, 0.1, 12), (0.1, 0.1, 0.3, 13),
+                 (0.9, 0.9, 0.9, 14), (0.6, 0.2, 0.9, 15)])
+    assert t.add_batch(cloud) == 0
+    assert t.deepen([1], min_points=2) == (False, 1)
+    t.sweep()
+    grids, offset = t.stats().num_grids, t.stats().persistent_offset
+    assert t.collapse([1, 1, 0, 9]) == (1, 3, 3)  # the root and a leaf are not twigs
+    t.sweep()
+    s = t.stats()
+    c1 = t.node(1)
+    assert c1.is_leaf and c1.num_points == 3 and c1.num_voxels == 0 and c1.grid < 0
+    assert sorted(t.leaf_points(1)[1]) == [0, 1, 2]
+    assert s.num_grids == grids - 1 and s.num_nodes == 17
+    more = pts([(0.2, 0.2, 0.2, 21), (0.2, 0.3, 0.2, 22), (0.3, 0.2, 0.3, 23), (0.1, 0.3, 0.3, 24)])
+    assert t.add_batch(more) == 0
+    t.sweep()
+    s2 = t.stats()
+    assert not t.node(1).is_leaf and t.node(1).grid >= 0
+    assert s2.num_grids == grids  # the pooled grid, not a new one
+    grid_bytes = 16 * ((128 ** 3 // 8 + 16) // 16)
+    assert s2.persistent_offset - offset < grid_bytes  # no grid charge beyond the chunks
+
+
+def test_deepen_is_refused_by_the_memory_check():
+    # the batch's memory check (remolod_octree.cu:1181-1210) stops a deepening
+    # pass too: nothing splits and the flag is raised
+    # a margin of 1 byte (0 means the default 200 MB); the root grid and the
+    # first batch's chunks take the store past 300,000 bytes
+    t = unit_tree(max_points_per_node=4, persistent_capacity=300000, safety_margin=1)
+    cloud = pts([(0.1, 0.1, 0.1, 11), (0.3, 0.1, 0.1, 12), (0.1, 0.1, 0.3, 13),
+                 (0.9, 0.9, 0.9, 14), (0.6, 0.2, 0.9, 15)])
+    assert t.add_batch(cloud) == 0
+    t.sweep()
+    n0 = t.stats().num_nodes
+    assert t.stats().persistent_offset >= 300000
+    assert t.deepen([1]) == (True, 0)
+    t.sweep()
+    assert t.stats().num_nodes == n0 and t.stats().mem_capacity_reached == 1

@@ -179,3 +179,31 @@ def test_collapse_undoes_deepening_and_matches_oracle(c1_cloud):
     compare_all(ctx, tree)
     ctx.close()
     tree.close()
+
+
+def test_deepen_is_refused_by_the_memory_check(c1_cloud):
+    """A store the memory check has already closed (230 MB: the build stops
+    after five of eight batches) refuses a deepening pass as it refuses a
+    batch: nothing splits, `stopped` is set, and the tree still equals the
+    oracle's, which refuses the same pass."""
+    from test_ref_pin import load
+    from gpu_helpers import build_gpu, build_oracle
+    from remobench_b200.lod import make_frame
+    cap = int(load("ref_config1_ieee_store230MB.npz")["persistent_capacity"])
+    cfg, cloud, bmin, bmax = c1_cloud
+    ctx, _ = build_gpu(cloud, bmin, bmax, cfg.batch_size, store_capacity=cap)
+    tree = build_oracle(cloud, bmin, bmax, cfg.batch_size, persistent_capacity=cap)
+    tree.accumulate(5)
+    assert ctx.stats().mem_capacity_reached == 1
+    f = make_frame(bmin, bmax, W, H, yaw=1.2, pitch=-0.5, radius_scale=0.5)
+    ctx.analyze(f, min_points=16, closure_margin=8, frontier_only=False, queue_capacity=4096)
+    queue = ctx.queue()
+    n0 = ctx.stats().num_nodes
+    d = ctx.refine_deepen(64)
+    assert d.stopped == 1 and d.nodes_selected == 0 and d.nodes_split == 0
+    assert tree.deepen(queue[:64]) == (True, 0)
+    tree.sweep()
+    assert ctx.stats().num_nodes == n0
+    compare_all(ctx, tree)
+    ctx.close()
+    tree.close()

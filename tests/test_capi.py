@@ -37,11 +37,13 @@ def test_abi_version_and_status_strings():
 
 
 STRUCTS = ["rb_kernel_profile", "rb_config", "rb_cloud_meta", "rb_batch_view", "rb_frame", "rb_build_result", "rb_stats",
-           "rb_render_result", "rb_accum_globals", "rb_accum", "rb_node_info", "rb_point"]
+           "rb_render_result", "rb_accum_globals", "rb_accum", "rb_node_info", "rb_point",
+           "rb_deepen_result", "rb_collapse_result", "rb_refine_result"]
 PY = {"rb_kernel_profile": capi.KernelProfile, "rb_config": capi.Config, "rb_cloud_meta": capi.CloudMeta, "rb_batch_view": capi.BatchView,
       "rb_frame": capi.Frame, "rb_build_result": capi.BuildResult, "rb_stats": capi.Stats,
       "rb_render_result": capi.RenderResult, "rb_accum_globals": capi.AccumGlobals, "rb_accum": capi.Accum,
-      "rb_node_info": capi.NodeInfo}
+      "rb_node_info": capi.NodeInfo, "rb_deepen_result": capi.DeepenResult,
+      "rb_collapse_result": capi.CollapseResult, "rb_refine_result": capi.RefineResult}
 
 
 def test_struct_layouts_match_header():
@@ -102,3 +104,11 @@ def test_product_path_has_no_cpu_fallback():
             if f.endswith((".py", ".cpp", ".cu", ".h", ".c")):
                 text = open(os.path.join(dirpath, f), errors="replace").read()
                 assert not pat.search(text), f
+
+
+def test_refinement_calls_reject_a_missing_context():
+    lib = capi.lib()
+    d, r = capi.DeepenResult(), capi.CollapseResult()
+    ids = (ctypes.c_uint32 * 2)(1, 2)
+    assert lib.rb_refine_deepen(None, 8, 0, ctypes.byref(d)) == capi.RB_ERR_INVALID_ARG
+    assert lib.rb_refine_collapse(None, ids, 2, 0, ctypes.byref(r)) == capi.RB_ERR_INVALID_ARG
